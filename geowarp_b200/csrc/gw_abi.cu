@@ -1,0 +1,634 @@
+// C ABI of the engine (declarations and reference citations in
+// include/geowarp_b200.h).  This is the library's single translation unit.
+#include <stddef.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "gw_step_kernels.cuh"
+#include "gw_krylov.cuh"
+
+using namespace gw;
+
+namespace {
+
+thread_local char g_msg[512];
+
+#define GW_CUDA(call)                                                                         \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            snprintf(g_msg, sizeof(g_msg), "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
+            return GW_ECUDA;                                                                  \
+        }                                                                                     \
+    } while (0)
+#define GW_LAUNCHED() GW_CUDA(cudaGetLastError())
+#define GW_REQUIRE(cond)                                                      \
+    do {                                                                      \
+        if (!(cond)) {                                                        \
+            snprintf(g_msg, sizeof(g_msg), "invalid argument: %s", #cond);    \
+            return GW_EINVAL;                                                 \
+        }                                                                     \
+    } while (0)
+
+inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+inline int red_grid_rows(int n_rows) { int b = nblk(n_rows, kThreads / 32); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
+inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
+
+LaunchConst make_lc(const gw_grid_t *g, const gw_material_t *m, const gw_step_t *st) {
+    LaunchConst c;
+    memset(&c, 0, sizeof(c));
+    c.g = *g;
+    if (st) c.st = *st;
+    if (m) {
+        c.mc = make_matconst(*m);
+        c.E0 = m->youngs_modulus;
+        c.nu = m->poisson_ratio;
+    }
+    return c;
+}
+
+int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
+
+// -------------------------------------------------------------- exclusive scan
+int64_t scan_ws_ints(int64_t n) {
+    int64_t total = 0;
+    while (n > 1024) {
+        const int64_t nb = (n + 1023) / 1024;
+        total += 2 * nb + 64;
+        n = nb;
+    }
+    return total + 64;
+}
+
+int scan_exclusive(const int *in, int *out, int n, int *ws, cudaStream_t s) {
+    if (n <= 0) return GW_OK;
+    const int nb = (n + 1023) / 1024;
+    int *sums = ws;
+    int *sums_scan = ws + nb;
+    k_scan_block<<<nb, 1024, 0, s>>>(in, out, n, nb > 1 ? sums : nullptr);
+    GW_LAUNCHED();
+    if (nb > 1) {
+        int rc = scan_exclusive(sums, sums_scan, nb, ws + 2 * nb + 64, s);
+        if (rc) return rc;
+        k_scan_add<<<nb, 1024, 0, s>>>(out, n, sums_scan);
+        GW_LAUNCHED();
+    }
+    return GW_OK;
+}
+
+__global__ void k_add2(const int *a, const int *b, int *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *out = *a + *b;
+}
+
+int n_cells_of(const gw_grid_t &g) {
+    int c = 1;
+    for (int k = 0; k < g.dim; ++k) c *= g.n_grid[k];
+    return c;
+}
+
+}  // namespace
+
+// ==================================================================== queries
+extern "C" int gw_version(void) { return 1; }
+
+extern "C" const char *gw_status_string(int code) {
+    switch (code) {
+        case GW_OK: return "ok";
+        case GW_EINVAL: return g_msg[0] ? g_msg : "invalid argument";
+        case GW_ECUDA: return g_msg[0] ? g_msg : "CUDA error";
+        case GW_ENOCONV: return "Krylov solver did not reach the tolerance";
+        case GW_EBREAKDOWN: return "Krylov breakdown";
+        case GW_ENAN: return "non-finite value";
+        case GW_ERANGE: return "particle support outside the background grid";
+        case GW_EMODEL: return "material model not available for this solver kind";
+        default: return "unknown status";
+    }
+}
+
+extern "C" int gw_read_device_status(int32_t *flag_host, void *stream) {
+    GW_REQUIRE(flag_host);
+    int v = 0;
+    GW_CUDA(cudaMemcpyFromSymbolAsync(&v, g_status, sizeof(int), 0, cudaMemcpyDeviceToHost, S(stream)));
+    GW_CUDA(cudaStreamSynchronize(S(stream)));
+    const int zero = 0;
+    GW_CUDA(cudaMemcpyToSymbolAsync(g_status, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, S(stream)));
+    GW_CUDA(cudaStreamSynchronize(S(stream)));
+    *flag_host = v;
+    return GW_OK;
+}
+
+// ==================================================================== sort
+extern "C" int64_t gw_sort_workspace_bytes(int32_t n) {
+    const int64_t nb = (n + kSortTile - 1) / kSortTile;
+    return align256(4 * (int64_t)n) * 2 + align256(4 * 256 * nb) + align256(4 * scan_ws_ints(256 * nb));
+}
+
+extern "C" int gw_cell_sort(const gw_grid_t *grid, const gw_particles_t *pt, int32_t *keys_out, int32_t *perm_out,
+                            void *workspace, void *stream) {
+    GW_REQUIRE(grid && pt && keys_out && perm_out && workspace);
+    const int n = pt->n;
+    if (n == 0) return GW_OK;
+    cudaStream_t s = S(stream);
+    const int nb = (n + kSortTile - 1) / kSortTile;
+    char *w = (char *)workspace;
+    int *kalt = (int *)w; w += align256(4 * (int64_t)n);
+    int *valt = (int *)w; w += align256(4 * (int64_t)n);
+    int *hist = (int *)w; w += align256(4 * 256 * (int64_t)nb);
+    int *sws = (int *)w;
+    if (grid->dim == 2) k_cell_keys<2><<<nblk(n, kThreads), kThreads, 0, s>>>(*grid, pt->x, pt->lp, n, keys_out, perm_out);
+    else k_cell_keys<3><<<nblk(n, kThreads), kThreads, 0, s>>>(*grid, pt->x, pt->lp, n, keys_out, perm_out);
+    GW_LAUNCHED();
+    const int ncell = n_cells_of(*grid);
+    int bits = 1;
+    while ((1 << bits) < ncell && bits < 31) ++bits;
+    const int passes = (bits + 7) / 8;
+    int *kin = keys_out, *vin = perm_out, *kout = kalt, *vout = valt;
+    for (int ps = 0; ps < passes; ++ps) {
+        const int shift = 8 * ps;
+        k_radix_hist<<<nb, kThreads, 0, s>>>(kin, n, shift, nb, hist);
+        GW_LAUNCHED();
+        int rc = scan_exclusive(hist, hist, 256 * nb, sws, s);
+        if (rc) return rc;
+        k_radix_scatter<<<nb, kThreads, 0, s>>>(kin, vin, n, shift, nb, hist, kout, vout);
+        GW_LAUNCHED();
+        int *t = kin; kin = kout; kout = t;
+        t = vin; vin = vout; vout = t;
+    }
+    if (kin != keys_out) {
+        GW_CUDA(cudaMemcpyAsync(keys_out, kin, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+        GW_CUDA(cudaMemcpyAsync(perm_out, vin, 4 * (size_t)n, cudaMemcpyDeviceToDevice, s));
+    }
+    return GW_OK;
+}
+
+// ==================================================================== activation / compaction / pattern
+extern "C" int gw_p2g_activate(const gw_grid_t *grid, const gw_particles_t *pt, const int32_t *perm,
+                               uint8_t *node_active, uint32_t *cell_span_u8, uint8_t *boundary, void *stream) {
+    GW_REQUIRE(grid && pt && node_active && cell_span_u8 && boundary);
+    if (pt->n == 0) return GW_OK;
+    LaunchConst c = make_lc(grid, nullptr, nullptr);
+    PtrsP p = make_ptrs(*pt);
+    uint32_t *cs = cell_span_u8;
+    const int b = nblk(pt->n, kThreads);
+    switch (grid->kind) {
+        case GW_KIND_SOLID2D: k_activate<GW_KIND_SOLID2D><<<b, kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
+        case GW_KIND_COUPLED2D: k_activate<GW_KIND_COUPLED2D><<<b, kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
+        case GW_KIND_COUPLED3D: k_activate<GW_KIND_COUPLED3D><<<b, kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
+        default: return GW_EINVAL;
+    }
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+extern "C" int gw_touched_nodes(const gw_grid_t *grid, const uint32_t *cell_span, uint8_t *touched, void *stream) {
+    GW_REQUIRE(grid && cell_span && touched);
+    const int nc = n_cells_of(*grid);
+    if (grid->dim == 2) k_touched<2><<<nblk(nc, kThreads), kThreads, 0, S(stream)>>>(*grid, cell_span, nc, touched);
+    else k_touched<3><<<nblk(nc, kThreads), kThreads, 0, S(stream)>>>(*grid, cell_span, nc, touched);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+extern "C" int64_t gw_scan_workspace_bytes(int32_t n) { return align256(4 * ((int64_t)n + 1)) + align256(4 * (scan_ws_ints((int64_t)n + 1) + 64)); }
+
+extern "C" int gw_compact_rows(const gw_grid_t *grid, const uint8_t *node_active, const uint8_t *boundary,
+                               int32_t *node2row, int32_t *row2node, uint8_t *free_mask, int32_t *n_rows_host,
+                               void *workspace, void *stream) {
+    GW_REQUIRE(grid && node_active && node2row && row2node && n_rows_host && workspace);
+    const int n = grid->n_nodes;
+    cudaStream_t s = S(stream);
+    char *w = (char *)workspace;
+    int *tmp = (int *)w; w += align256(4 * ((int64_t)n + 1));
+    int *sws = (int *)w;
+    k_flags_to_int<<<nblk(n, kThreads), kThreads, 0, s>>>(node_active, n, tmp);
+    GW_LAUNCHED();
+    int *last = sws;  // [0]: flag of the last node, [1]: number of active nodes
+    GW_CUDA(cudaMemcpyAsync(last, tmp + (n - 1), 4, cudaMemcpyDeviceToDevice, s));
+    int rc = scan_exclusive(tmp, tmp, n, sws + 64, s);
+    if (rc) return rc;
+    k_compact<<<nblk(n, kThreads), kThreads, 0, s>>>(node_active, tmp, n, grid->nf, boundary, node2row, row2node,
+                                                     free_mask);
+    GW_LAUNCHED();
+    k_add2<<<1, 32, 0, s>>>(tmp + (n - 1), last, last + 1);
+    GW_LAUNCHED();
+    int tot = 0;
+    GW_CUDA(cudaMemcpyAsync(&tot, last + 1, 4, cudaMemcpyDeviceToHost, s));
+    GW_CUDA(cudaStreamSynchronize(s));
+    *n_rows_host = tot;
+    return GW_OK;
+}
+
+extern "C" int gw_pattern_count(const gw_grid_t *grid, const uint32_t *cell_span_u8, const int32_t *node2row,
+                                const int32_t *row2node, int32_t n_rows, uint32_t *stencil, int32_t *row_ptr,
+                                int32_t *nnzb_host, void *workspace, void *stream) {
+    GW_REQUIRE(grid && cell_span_u8 && node2row && row2node && stencil && row_ptr && nnzb_host && workspace);
+    cudaStream_t s = S(stream);
+    const uint32_t *cs = cell_span_u8;
+    const int mw = grid->dim == 2 ? 1 : 4;
+    GW_CUDA(cudaMemsetAsync(row_ptr, 0, 4 * ((size_t)n_rows + 1), s));
+    if (n_rows > 0) {
+        if (grid->dim == 2)
+            k_pattern_count<2><<<nblk(n_rows, kThreads), kThreads, 0, s>>>(*grid, cs, node2row, row2node, n_rows, mw, stencil, row_ptr);
+        else
+            k_pattern_count<3><<<nblk(n_rows, kThreads), kThreads, 0, s>>>(*grid, cs, node2row, row2node, n_rows, mw, stencil, row_ptr);
+        GW_LAUNCHED();
+    }
+    int rc = scan_exclusive(row_ptr, row_ptr, n_rows + 1, (int *)workspace, s);
+    if (rc) return rc;
+    int tot = 0;
+    GW_CUDA(cudaMemcpyAsync(&tot, row_ptr + n_rows, 4, cudaMemcpyDeviceToHost, s));
+    GW_CUDA(cudaStreamSynchronize(s));
+    *nnzb_host = tot;
+    return GW_OK;
+}
+
+extern "C" int gw_pattern_fill(const gw_grid_t *grid, const gw_bsr_t *A, int32_t *cols, void *stream) {
+    GW_REQUIRE(grid && A && cols);
+    if (A->n_rows == 0) return GW_OK;
+    PtrsA a = make_ptrs(*A);
+    if (grid->dim == 2) k_pattern_fill<2><<<nblk(A->n_rows, kThreads), kThreads, 0, S(stream)>>>(*grid, a, cols);
+    else k_pattern_fill<3><<<nblk(A->n_rows, kThreads), kThreads, 0, S(stream)>>>(*grid, a, cols);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+// ==================================================================== consistent mass
+extern "C" int gw_mass_assemble(const gw_grid_t *grid, const gw_particles_t *pt, const int32_t *perm,
+                                const gw_step_t *st, const gw_bsr_t *M, double *rhs, void *stream) {
+    GW_REQUIRE(grid && pt && perm && st && M && rhs && M->nf == 1);
+    cudaStream_t s = S(stream);
+    GW_CUDA(cudaMemsetAsync(M->vals, 0, sizeof(double) * (size_t)M->nnzb, s));
+    GW_CUDA(cudaMemsetAsync(rhs, 0, sizeof(double) * (size_t)M->n_rows, s));
+    LaunchConst c = make_lc(grid, nullptr, st);
+    PtrsP p = make_ptrs(*pt);
+    PtrsA m = make_ptrs(*M);
+    const int b = nblk(pt->n, kThreads);
+    if (pt->n > 0) {
+        if (grid->kind == GW_KIND_COUPLED2D) k_mass<GW_KIND_COUPLED2D><<<b, kThreads, 0, s>>>(c, p, perm, m, rhs);
+        else if (grid->kind == GW_KIND_COUPLED3D) k_mass<GW_KIND_COUPLED3D><<<b, kThreads, 0, s>>>(c, p, perm, m, rhs);
+        else return GW_EINVAL;
+        GW_LAUNCHED();
+    }
+    if (M->n_rows > 0) {
+        if (grid->dim == 2) k_mass_fix<2><<<nblk(M->n_rows, kThreads), kThreads, 0, s>>>(m);
+        else k_mass_fix<3><<<nblk(M->n_rows, kThreads), kThreads, 0, s>>>(m);
+        GW_LAUNCHED();
+    }
+    return GW_OK;
+}
+
+extern "C" int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_row2node, int32_t n_mass_rows,
+                                     const double *p_hat, const uint8_t *boundary, const uint8_t *node_active,
+                                     double *u_old, double *u_new, void *stream) {
+    GW_REQUIRE(grid && mass_row2node && p_hat && boundary && u_old && u_new);
+    if (n_mass_rows == 0) return GW_OK;
+    k_set_nodal_pressure<<<nblk(n_mass_rows, kThreads), kThreads, 0, S(stream)>>>(
+        n_mass_rows, mass_row2node, p_hat, boundary, grid->kind == GW_KIND_COUPLED3D ? node_active : nullptr,
+        grid->n_nodes, grid->nf, u_old, u_new);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+// ==================================================================== residual + Jacobian
+namespace {
+template <int KIND>
+int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
+                    const double *uo, const gw_bsr_t *A, int prec, double *R, double *force, const PtrsA &a,
+                    cudaStream_t s) {
+    const int b = nblk(p.n, kThreads);
+    if (p.n > 0) {
+        if (!A) k_assemble<KIND, false, double><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        else if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        else k_assemble<KIND, true, float><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        GW_LAUNCHED();
+    }
+    if (A && A->n_rows > 0) {
+        const int D = KindTraits<KIND>::D;
+        if (prec == GW_PREC_F64) k_identity_dirichlet<D, double><<<nblk(A->n_rows, kThreads), kThreads, 0, s>>>(a, fm);
+        else k_identity_dirichlet<D, float><<<nblk(A->n_rows, kThreads), kThreads, 0, s>>>(a, fm);
+        GW_LAUNCHED();
+    }
+    return GW_OK;
+}
+}  // namespace
+
+extern "C" int gw_assemble(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
+                           const gw_particles_t *pt, const int32_t *perm, const uint8_t *free_mask,
+                           const double *u_new, const double *u_old, const gw_bsr_t *A, int32_t prec, double *R_rows,
+                           double *force, void *stream) {
+    GW_REQUIRE(grid && mat && st && pt && perm && free_mask && u_new && u_old && R_rows);
+    GW_REQUIRE(mat->model >= 0 && mat->model <= GW_MODEL_NORSAND);
+    cudaStream_t s = S(stream);
+    LaunchConst c = make_lc(grid, mat, st);
+    PtrsP p = make_ptrs(*pt);
+    gw_bsr_t dummy;
+    memset(&dummy, 0, sizeof(dummy));
+    // the row map and stencil are needed for the residual even without a matrix
+    PtrsA a = make_ptrs(A ? *A : dummy);
+    if (A) {
+        const size_t vb = (prec == GW_PREC_F64 ? 8 : 4) * (size_t)A->nnzb * A->nf * A->nf;
+        GW_CUDA(cudaMemsetAsync(A->vals, 0, vb, s));
+        GW_CUDA(cudaMemsetAsync(R_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
+    }
+    switch (grid->kind) {
+        case GW_KIND_SOLID2D: return launch_assemble<GW_KIND_SOLID2D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
+        case GW_KIND_COUPLED2D: return launch_assemble<GW_KIND_COUPLED2D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
+        case GW_KIND_COUPLED3D: return launch_assemble<GW_KIND_COUPLED3D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
+        default: return GW_EINVAL;
+    }
+}
+
+// ==================================================================== Krylov
+namespace {
+struct KWs {
+    double *r, *rh, *p, *v, *y, *s, *z, *t, *Minv, *partials;
+    KScalars *sc;
+};
+
+int64_t krylov_ws_bytes(int64_t n_rows, int nf) {
+    const int64_t n = n_rows * nf;
+    return 8 * align256(8 * n) + align256(8 * n_rows * nf * nf) + align256(8 * (int64_t)kRedBlocks * 4) +
+           align256(sizeof(KScalars));
+}
+
+KWs carve(void *ws, int64_t n_rows, int nf) {
+    const int64_t n = n_rows * nf;
+    char *w = (char *)ws;
+    KWs k;
+    double **vecs[8] = {&k.r, &k.rh, &k.p, &k.v, &k.y, &k.s, &k.z, &k.t};
+    for (int i = 0; i < 8; ++i) { *vecs[i] = (double *)w; w += align256(8 * n); }
+    k.Minv = (double *)w; w += align256(8 * n_rows * nf * nf);
+    k.partials = (double *)w; w += align256(8 * (int64_t)kRedBlocks * 4);
+    k.sc = (KScalars *)w;
+    return k;
+}
+
+template <int NF, typename VT>
+int krylov(const gw_bsr_t *A, int method, int precond, const double *b, double *x, double rtol, int max_iter, void *ws,
+           int *iters, double *relres, cudaStream_t s) {
+    PtrsA a = make_ptrs(*A);
+    KWs k = carve(ws, A->n_rows, NF);
+    const int D = (A->mask_words == 1) ? 2 : 3;
+    const int nr = A->n_rows;
+    if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
+    BicgVecs V;
+    V.x = x; V.b = b; V.r = k.r; V.rh = k.rh; V.p = k.p; V.v = k.v; V.y = k.y; V.s = k.s; V.z = k.z; V.t = k.t;
+    V.Minv = k.Minv; V.partials = k.partials; V.sc = k.sc;
+    GW_CUDA(cudaMemsetAsync(k.sc, 0, sizeof(KScalars), s));
+    KScalars h;
+    memset(&h, 0, sizeof(h));
+    h.max_iter = max_iter;
+    GW_CUDA(cudaMemcpyAsync(&k.sc->max_iter, &h.max_iter, sizeof(int), cudaMemcpyHostToDevice, s));
+    k_precond_setup<NF, VT><<<nblk(nr, kThreads), kThreads, 0, s>>>(a, D, precond, k.Minv);
+    GW_LAUNCHED();
+    const int gw_rows = red_grid_rows(nr), ge_rows = red_grid_elems(nr);
+    if (method == GW_KRYLOV_CG) k_cg_init<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V, rtol);
+    else k_bicg_init<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V, rtol);
+    GW_LAUNCHED();
+    int chunk = 2;
+    for (;;) {
+        GW_CUDA(cudaMemcpyAsync(&h, k.sc, sizeof(KScalars), cudaMemcpyDeviceToHost, s));
+        GW_CUDA(cudaStreamSynchronize(s));
+        if (h.done) break;
+        for (int it = 0; it < chunk; ++it) {
+            if (method == GW_KRYLOV_CG) {
+                k_cg_p<NF><<<red_grid_elems((int64_t)nr * NF), kThreads, 0, s>>>(nr, V);
+                k_cg_q<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V);
+                k_cg_xr<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
+            } else {
+                k_bicg_p<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
+                k_bicg_v<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V);
+                k_bicg_s<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
+                k_bicg_t<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V);
+                k_bicg_xr<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
+            }
+        }
+        GW_LAUNCHED();
+        chunk = chunk < 64 ? chunk * 2 : 64;
+    }
+    *iters = h.iters;
+    *relres = (h.bb > 0.0) ? ::sqrt(h.rr / h.bb) : 0.0;
+    if (h.status == ST_BREAKDOWN) return GW_EBREAKDOWN;
+    if (h.status == ST_NAN) return GW_ENAN;
+    if (h.rr > h.tol2) return GW_ENOCONV;
+    return GW_OK;
+}
+
+template <typename VT>
+int krylov_nf(const gw_bsr_t *A, int method, int precond, const double *b, double *x, double rtol, int max_iter,
+              void *ws, int *iters, double *relres, cudaStream_t s) {
+    switch (A->nf) {
+        case 1: return krylov<1, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
+        case 2: return krylov<2, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
+        case 3: return krylov<3, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
+        case 4: return krylov<4, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
+        default: return GW_EINVAL;
+    }
+}
+}  // namespace
+
+namespace {
+int64_t gmres_ws_bytes(int64_t n_rows, int nf, int restart) {
+    const int64_t n = n_rows * nf;
+    return align256(8 * n * (restart + 1)) + 2 * align256(8 * n) + align256(8 * n_rows * nf * nf) +
+           align256(8 * (int64_t)kRedBlocks * (kGmresMaxRestart + 1)) + align256(sizeof(GScalars));
+}
+
+template <int NF, typename VT>
+int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rtol, int max_iter, int restart,
+          void *ws, int *iters, double *relres, cudaStream_t s) {
+    PtrsA a = make_ptrs(*A);
+    const int nr = A->n_rows;
+    if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
+    const int64_t n = (int64_t)nr * NF;
+    char *w = (char *)ws;
+    GmresVecs G;
+    G.V = (double *)w; w += align256(8 * n * (restart + 1));
+    G.w = (double *)w; w += align256(8 * n);
+    G.z = (double *)w; w += align256(8 * n);
+    G.Minv = (double *)w; w += align256(8 * (int64_t)nr * NF * NF);
+    G.partials = (double *)w; w += align256(8 * (int64_t)kRedBlocks * (kGmresMaxRestart + 1));
+    G.sc = (GScalars *)w;
+    G.x = x; G.b = b; G.n = (size_t)n;
+    const size_t head = offsetof(GScalars, H);
+    GW_CUDA(cudaMemsetAsync(G.sc, 0, head, s));
+    struct { int max_iter, restart; } lim = {max_iter, restart};
+    GW_CUDA(cudaMemcpyAsync(&G.sc->max_iter, &lim, sizeof(lim), cudaMemcpyHostToDevice, s));
+    const int D = (A->mask_words == 1) ? 2 : 3;
+    k_precond_setup<NF, VT><<<nblk(nr, kThreads), kThreads, 0, s>>>(a, D, precond, G.Minv);
+    GW_LAUNCHED();
+    const int gr = red_grid_rows(nr), ge = red_grid_elems(nr), gv = red_grid_elems(n);
+    GScalars h;
+    memset(&h, 0, head);
+    int first = 1;
+    for (int cycle = 0; cycle < 1000000; ++cycle) {
+        k_gm_residual<NF, VT><<<gr, kThreads, 0, s>>>(a, G, first, rtol);
+        k_gm_next<NF><<<ge, kThreads, 0, s>>>(nr, G, 1);
+        GW_LAUNCHED();
+        first = 0;
+        GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
+        GW_CUDA(cudaStreamSynchronize(s));
+        if (h.done) break;
+        int chunk = 4;
+        for (;;) {
+            for (int it = 0; it < chunk; ++it) {
+                k_gm_spmv<NF, VT><<<gr, kThreads, 0, s>>>(a, G);
+                k_gm_dots<<<gv, kThreads, 0, s>>>(G, 0);
+                k_gm_update<<<gv, kThreads, 0, s>>>(G, 0);
+                k_gm_dots<<<gv, kThreads, 0, s>>>(G, 1);
+                k_gm_update<<<gv, kThreads, 0, s>>>(G, 1);
+                k_gm_next<NF><<<ge, kThreads, 0, s>>>(nr, G, 0);
+            }
+            GW_LAUNCHED();
+            GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
+            GW_CUDA(cudaStreamSynchronize(s));
+            if (h.cycle_done) break;
+            chunk = chunk < 32 ? chunk * 2 : 32;
+        }
+        if (h.status) break;
+        k_gm_solve_y<<<1, 32, 0, s>>>(G.sc);
+        k_gm_update_x<NF><<<ge, kThreads, 0, s>>>(nr, G);
+        GW_LAUNCHED();
+    }
+    *iters = h.iters;
+    *relres = (h.bnorm > 0.0) ? h.resid / h.bnorm : 0.0;
+    if (h.status == ST_NAN) return GW_ENAN;
+    if (h.resid > h.tol) return GW_ENOCONV;
+    return GW_OK;
+}
+
+template <typename VT>
+int gmres_nf(const gw_bsr_t *A, int precond, const double *b, double *x, double rtol, int max_iter, int restart,
+             void *ws, int *iters, double *relres, cudaStream_t s) {
+    switch (A->nf) {
+        case 1: return gmres<1, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
+        case 2: return gmres<2, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
+        case 3: return gmres<3, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
+        case 4: return gmres<4, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
+        default: return GW_EINVAL;
+    }
+}
+}  // namespace
+
+extern "C" int64_t gw_gmres_workspace_bytes(int32_t n_rows, int32_t nf, int32_t restart) {
+    if (restart < 1 || restart > kGmresMaxRestart) return -1;
+    return gmres_ws_bytes(n_rows, nf, restart);
+}
+
+extern "C" int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const double *b, double *x,
+                                  double rtol, int32_t max_iter, int32_t restart, void *workspace, int32_t *iters_host,
+                                  double *relres_host, void *stream) {
+    GW_REQUIRE(A && b && x && workspace && iters_host && relres_host && max_iter > 0);
+    GW_REQUIRE(restart >= 1 && restart <= kGmresMaxRestart);
+    int it = 0;
+    double rr = 0.0;
+    int rc = (prec == GW_PREC_F64)
+                 ? gmres_nf<double>(A, precond, b, x, rtol, max_iter, restart, workspace, &it, &rr, S(stream))
+                 : gmres_nf<float>(A, precond, b, x, rtol, max_iter, restart, workspace, &it, &rr, S(stream));
+    *iters_host = it;
+    *relres_host = rr;
+    return rc;
+}
+
+extern "C" int64_t gw_krylov_workspace_bytes(int32_t n_rows, int32_t nf, int32_t prec) {
+    (void)prec;
+    return krylov_ws_bytes(n_rows, nf);
+}
+
+extern "C" int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond, const double *b,
+                                   double *x, double rtol, int32_t max_iter, void *workspace, int32_t *iters_host,
+                                   double *relres_host, void *stream) {
+    GW_REQUIRE(A && b && x && workspace && iters_host && relres_host && max_iter > 0);
+    int it = 0;
+    double rr = 0.0;
+    int rc = (prec == GW_PREC_F64)
+                 ? krylov_nf<double>(A, method, precond, b, x, rtol, max_iter, workspace, &it, &rr, S(stream))
+                 : krylov_nf<float>(A, method, precond, b, x, rtol, max_iter, workspace, &it, &rr, S(stream));
+    *iters_host = it;
+    *relres_host = rr;
+    return rc;
+}
+
+namespace {
+template <typename VT>
+int spmv_any(const gw_bsr_t *A, const double *x, double *y, bool trans, cudaStream_t s) {
+    PtrsA a = make_ptrs(*A);
+    const int g = red_grid_rows(A->n_rows);
+    if (A->n_rows == 0) return GW_OK;
+    if (trans) GW_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
+#define GW_SPMV_CASE(NF_)                                                  \
+    case NF_:                                                              \
+        if (trans) k_spmv_t<NF_, VT><<<g, kThreads, 0, s>>>(a, x, y);      \
+        else k_spmv<NF_, VT><<<g, kThreads, 0, s>>>(a, x, y);              \
+        break;
+    switch (A->nf) {
+        GW_SPMV_CASE(1) GW_SPMV_CASE(2) GW_SPMV_CASE(3) GW_SPMV_CASE(4)
+        default: return GW_EINVAL;
+    }
+#undef GW_SPMV_CASE
+    GW_LAUNCHED();
+    return GW_OK;
+}
+}  // namespace
+
+extern "C" int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream) {
+    GW_REQUIRE(A && x && y);
+    return prec == GW_PREC_F64 ? spmv_any<double>(A, x, y, false, S(stream)) : spmv_any<float>(A, x, y, false, S(stream));
+}
+
+extern "C" int gw_bsr_spmv_t(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream) {
+    GW_REQUIRE(A && x && y);
+    return prec == GW_PREC_F64 ? spmv_any<double>(A, x, y, true, S(stream)) : spmv_any<float>(A, x, y, true, S(stream));
+}
+
+extern "C" int gw_norm2(const double *v, int32_t n, double *norm_dev, void *workspace, void *stream) {
+    GW_REQUIRE(v && norm_dev && workspace);
+    double *partials = (double *)workspace;
+    unsigned *ticket = (unsigned *)((char *)workspace + align256(8 * kRedBlocks));
+    GW_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), S(stream)));
+    k_norm2<<<red_grid_elems(n), kThreads, 0, S(stream)>>>(v, n, partials, ticket, norm_dev);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+extern "C" int gw_apply_increment(const gw_bsr_t *A, const double *delta, double *u_full, void *stream) {
+    GW_REQUIRE(A && delta && u_full);
+    if (A->n_rows == 0) return GW_OK;
+    k_apply_increment<<<nblk(A->n_rows, kThreads), kThreads, 0, S(stream)>>>(A->n_rows, A->nf, A->row2node, delta, u_full);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+// ==================================================================== G2P
+extern "C" int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_particles_t *pt, const double *u_new,
+                      const double *u_old, void *stream) {
+    GW_REQUIRE(grid && st && pt && u_new && u_old);
+    if (pt->n == 0) return GW_OK;
+    LaunchConst c = make_lc(grid, nullptr, st);
+    PtrsP p = make_ptrs(*pt);
+    const int b = nblk(pt->n, kThreads);
+    switch (grid->kind) {
+        case GW_KIND_SOLID2D: k_g2p<GW_KIND_SOLID2D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
+        case GW_KIND_COUPLED2D: k_g2p<GW_KIND_COUPLED2D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
+        case GW_KIND_COUPLED3D: k_g2p<GW_KIND_COUPLED3D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
+        default: return GW_EINVAL;
+    }
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+// ==================================================================== single-point models
+extern "C" int gw_return_map(const gw_material_t *mat, int32_t n, const double *e_trial, const double *eps_v_total,
+                             const double *pi_old, double *pi_new, double *e_out, double *tau_out,
+                             double *dtau_de_out, void *stream) {
+    GW_REQUIRE(mat && e_trial && e_out && tau_out);
+    if (n == 0) return GW_OK;
+    MatConst mc = make_matconst(*mat);
+    const double nu = mat->poisson_ratio, E = mat->youngs_modulus;
+    const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = E / (2.0 * (1.0 + nu));
+    k_return_map<<<nblk(n, kThreads), kThreads, 0, S(stream)>>>(mc, lam, mu, n, e_trial, eps_v_total, pi_old, pi_new,
+                                                                e_out, tau_out, dtau_de_out);
+    GW_LAUNCHED();
+    return GW_OK;
+}

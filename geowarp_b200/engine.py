@@ -1,0 +1,437 @@
+"""Device-resident implicit cpGIMP engine (one problem instance, one GPU).
+
+The Engine owns every device buffer (torch tensors used as plain CUDA memory)
+and sequences one load step through the C ABI of libgeowarp_b200.so:
+
+    reset -> [user BCs] -> cell sort -> P2G activation (+ pressure BCs)
+          -> [u-p: consistent-mass projection, CG on the GPU]
+          -> row compaction -> block-CSR pattern (once per step)
+          -> Newton { residual + element tangent, ||R||, Krylov, u += delta }
+          -> G2P + lp update
+
+which is the order of advance_one_step in solvers/quasi_static_solver_2d.py:239-258,
+solvers/quasi_static_coupled_solver_2d.py:274-313 and
+solvers/quasi_static_coupled_solver_3d.py:258-420.  There is no CPU path: every
+numerical step is a CUDA kernel of the library.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+import torch
+
+from . import _lib as L
+
+MODEL_IDS = {
+    "Hencky elasticity": L.MODEL_HENCKY,
+    "J2": L.MODEL_J2,
+    "Neo-Hookean": L.MODEL_NEOHOOKEAN,
+    "Linear elasticity": L.MODEL_LINEAR,
+    "Drucker-Prager": L.MODEL_DP,
+    "NorSand": L.MODEL_NORSAND,
+}
+
+PRECISIONS = {"fp64": L.PREC_F64, "mixed": L.PREC_F32}
+PRECONDS = {"diag": L.PRECOND_DIAG, "block": L.PRECOND_BLOCK}
+
+
+def _p(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def material_struct(mat):
+    """gw_material_t from a reference-style material dict."""
+    m = L.Material()
+    name = mat["material_name"]
+    if name not in MODEL_IDS:
+        raise ValueError(f"Unimplemented material model: {name}")
+    m.model = MODEL_IDS[name]
+    m.youngs_modulus = float(mat.get("youngs_modulus", 0.0))
+    m.poisson_ratio = float(mat.get("poisson_ratio", 0.0))
+    m.kappa = float(mat.get("kappa", 0.0))
+    m.friction_angle = float(mat.get("friction_angle", 0.0))
+    m.dilation_angle = float(mat.get("dilation_angle", 0.0))
+    m.cohesion = float(mat.get("cohesion", 0.0))
+    m.shape_factor = float(mat.get("shape_factor", 0.0))
+    m.dp_tension_cutoff = 1 if mat.get("tension_cutoff", True) else 0
+    m.ns_kappa = float(mat.get("kappa", 0.0)) if name == "NorSand" else 0.0
+    for key, attr in (("tilde_lambda", "ns_tilde_lambda"), ("M", "ns_M"), ("N", "ns_N"), ("beta", "ns_beta"),
+                      ("vc0", "ns_vc0"), ("p0", "ns_p0"), ("v0", "ns_v0"), ("h", "ns_h"),
+                      ("shear_modulus", "ns_shear_modulus"), ("initial_volumetric_strain", "ns_eps_v0")):
+        setattr(m, attr, float(mat.get(key, 0.0)))
+    if name == "NorSand" and m.ns_beta == 0.0:
+        m.ns_beta = 1.0
+    return m
+
+
+class _Buf:
+    """Grow-only device byte buffer."""
+
+    def __init__(self, device):
+        self.device = device
+        self.t = torch.empty(0, dtype=torch.uint8, device=device)
+
+    def get(self, nbytes):
+        nbytes = max(int(nbytes), 256)
+        if self.t.numel() < nbytes:
+            self.t = torch.empty(int(nbytes * 1.25) + 256, dtype=torch.uint8, device=self.device)
+        return self.t
+
+
+class Engine:
+    """State and step sequencing for one problem.
+
+    kind: 'solid2d' | 'coupled2d' | 'coupled3d'
+    n_grid: cells per axis; h: cell sizes used by the shape functions (2D
+    reference solvers use dx on both axes); h_nodes: cell sizes for nodal
+    positions; domain_min/max: lp clipping box.
+    """
+
+    KINDS = {"solid2d": L.KIND_SOLID2D, "coupled2d": L.KIND_COUPLED2D, "coupled3d": L.KIND_COUPLED3D}
+
+    def __init__(self, kind, n_grid, h, h_nodes, domain_min, domain_max, x_init, device=None,
+                 precision="fp64", precond="block", krylov_rtol=None, krylov_max_iter=20000, krylov="gmres",
+                 restart=100):
+        if not torch.cuda.is_available():
+            raise RuntimeError("geowarp_b200 needs a CUDA device (there is no CPU fallback)")
+        L.load()
+        self.kind_name = kind
+        self.kind = self.KINDS[kind]
+        self.D = 2 if kind != "coupled3d" else 3
+        self.nf = {"solid2d": 2, "coupled2d": 3, "coupled3d": 4}[kind]
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.n_grid = tuple(int(v) for v in n_grid)
+        self.n_nodes = int(np.prod([v + 1 for v in self.n_grid]))
+        self.n_cells = int(np.prod(self.n_grid))
+        self.h = tuple(float(v) for v in h)
+        self.h_nodes = tuple(float(v) for v in h_nodes)
+        self.domain_min = tuple(float(v) for v in domain_min)
+        self.domain_max = tuple(float(v) for v in domain_max)
+        self.precision = precision
+        self.prec = PRECISIONS[precision]
+        self.precond = PRECONDS[precond]
+        self.krylov_rtol = krylov_rtol if krylov_rtol is not None else (1e-12 if precision == "fp64" else 1e-6)
+        self.krylov_max_iter = krylov_max_iter
+        if krylov not in ("gmres", "bicgstab"):
+            raise ValueError(f"unknown Krylov method {krylov!r}")
+        self.krylov_method = krylov
+        self.restart = int(restart)
+        self.mw = 1 if self.D == 2 else 4
+
+        dev = self.device
+        f64 = dict(dtype=torch.float64, device=dev)
+        x = torch.as_tensor(np.asarray(x_init, dtype=np.float64)).to(dev)
+        self.N = x.shape[0]
+        N = self.N
+        self.x = x.contiguous()
+        self.x0 = x.clone()
+        self.lp = torch.zeros((N, self.D), **f64)
+        ident = torch.tensor([[1.0 + 1e-7, 0, 0], [0, 1.0 - 1e-6, 0], [0, 0, 1.0]], **f64)
+        self.F_old = ident.expand(N, 3, 3).contiguous()
+        self.F_new = self.F_old.clone()
+        self.b_old = self.F_old.clone()
+        self.b_new = self.F_old.clone()
+        self.sigma = torch.zeros((N, 3, 3), **f64)
+        self.pressure = torch.zeros(N, **f64)
+        self.pi_old = torch.zeros(N, **f64)
+        self.pi_new = torch.zeros(N, **f64)
+        self.ext_flag = torch.zeros(N, dtype=torch.bool, device=dev)
+        self.trac_flag = torch.zeros(N, dtype=torch.bool, device=dev)
+        self.pbc_flag = torch.zeros(N, dtype=torch.bool, device=dev)
+        self.E = None  # optional per-particle Young's modulus [N]
+
+        nn = self.n_nodes
+        self.boundary = torch.zeros(self.nf * nn, dtype=torch.bool, device=dev)
+        self.node_active = torch.zeros(nn, dtype=torch.uint8, device=dev)
+        self.cell_span = torch.zeros(self.n_cells, dtype=torch.int32, device=dev)
+        self.free_mask = torch.zeros(nn, dtype=torch.uint8, device=dev)
+        self.node2row = torch.zeros(nn, dtype=torch.int32, device=dev)
+        self.row2node = torch.zeros(nn, dtype=torch.int32, device=dev)
+        self.stencil = torch.zeros(nn * self.mw, dtype=torch.int32, device=dev)
+        self.u_new = torch.zeros(nn * self.nf, **f64)
+        self.u_old = torch.zeros(nn * self.nf, **f64)
+        self.keys = torch.zeros(N, dtype=torch.int32, device=dev)
+        self.perm = torch.zeros(N, dtype=torch.int32, device=dev)
+        self.force = torch.zeros(1, **f64)
+        self.norm_dev = torch.zeros(1, **f64)
+        self._sort_ws = _Buf(dev)
+        self._scan_ws = _Buf(dev)
+        self._kry_ws = _Buf(dev)
+        self._norm_ws = torch.zeros(16384, dtype=torch.uint8, device=dev)
+        self._row_ptr = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._cols = torch.zeros(1, dtype=torch.int32, device=dev)
+        self._vals = _Buf(dev)
+        self._R = torch.zeros(1, **f64)
+        self._delta = torch.zeros(1, **f64)
+        # consistent-mass system (u-p kinds)
+        if self.nf > self.D:
+            self.touched = torch.zeros(nn, dtype=torch.uint8, device=dev)
+            self.m_node2row = torch.zeros(nn, dtype=torch.int32, device=dev)
+            self.m_row2node = torch.zeros(nn, dtype=torch.int32, device=dev)
+            self.m_stencil = torch.zeros(nn * self.mw, dtype=torch.int32, device=dev)
+            self._m_row_ptr = torch.zeros(1, dtype=torch.int32, device=dev)
+            self._m_cols = torch.zeros(1, dtype=torch.int32, device=dev)
+            self._m_vals = torch.zeros(1, **f64)
+            self._m_rhs = torch.zeros(1, **f64)
+            self._m_x = torch.zeros(1, **f64)
+        self.n_rows = 0
+        self.nnzb = 0
+        self.m_rows = 0
+        self.m_nnzb = 0
+        self.step_params = {}
+        self.log = []  # per Newton iteration: (step, it, ||R||, krylov iters, relres, status)
+
+    # ------------------------------------------------------------------ structs
+    def grid_struct(self):
+        g = L.Grid()
+        g.dim = self.D
+        g.kind = self.kind
+        g.nf = self.nf
+        for k in range(3):
+            g.n_grid[k] = self.n_grid[k] if k < self.D else 0
+            g.h[k] = self.h[k] if k < self.D else 1.0
+            g.inv_h[k] = 1.0 / self.h[k] if k < self.D else 1.0
+            g.h_nodes[k] = self.h_nodes[k] if k < self.D else 1.0
+            g.domain_min[k] = self.domain_min[k] if k < self.D else 0.0
+            g.domain_max[k] = self.domain_max[k] if k < self.D else 0.0
+        g.n_nodes = self.n_nodes
+        return g
+
+    def particles_struct(self):
+        p = L.Particles()
+        p.n = self.N
+        p.x, p.x0, p.lp = _p(self.x), _p(self.x0), _p(self.lp)
+        p.F_old, p.F_new, p.b_old, p.b_new = _p(self.F_old), _p(self.F_new), _p(self.b_old), _p(self.b_new)
+        p.sigma, p.pressure, p.pi_old, p.pi_new = _p(self.sigma), _p(self.pressure), _p(self.pi_old), _p(self.pi_new)
+        p.ext_flag, p.trac_flag, p.pbc_flag = _p(self.ext_flag), _p(self.trac_flag), _p(self.pbc_flag)
+        p.E = _p(self.E)
+        return p
+
+    def bsr_struct(self, mass=False):
+        b = L.Bsr()
+        if mass:
+            b.n_rows, b.nf, b.nnzb, b.mask_words = self.m_rows, 1, self.m_nnzb, self.mw
+            b.row_ptr, b.cols, b.row2node, b.node2row = (_p(self._m_row_ptr), _p(self._m_cols), _p(self.m_row2node),
+                                                         _p(self.m_node2row))
+            b.stencil, b.vals = _p(self.m_stencil), _p(self._m_vals)
+        else:
+            b.n_rows, b.nf, b.nnzb, b.mask_words = self.n_rows, self.nf, self.nnzb, self.mw
+            b.row_ptr, b.cols, b.row2node, b.node2row = (_p(self._row_ptr), _p(self._cols), _p(self.row2node),
+                                                         _p(self.node2row))
+            b.stencil, b.vals = _p(self.stencil), _p(self._vals.t)
+        return b
+
+    @property
+    def stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    # ------------------------------------------------------------------ step pieces
+    def reset(self, clear_boundary):
+        self.u_old.zero_()
+        self.u_new.zero_()
+        self.node_active.zero_()
+        self.cell_span.zero_()
+        if clear_boundary:
+            self.boundary.zero_()
+
+    def sort_and_activate(self):
+        g, pt, s = self.grid_struct(), self.particles_struct(), self.stream
+        ws = self._sort_ws.get(L.load().gw_sort_workspace_bytes(self.N))
+        L.call("gw_cell_sort", C.byref(g), C.byref(pt), _p(self.keys), _p(self.perm), _p(ws), s)
+        L.call("gw_p2g_activate", C.byref(g), C.byref(pt), _p(self.perm), _p(self.node_active), _p(self.cell_span),
+               _p(self.boundary), s)
+
+    def _scan_ws_for(self, n):
+        return self._scan_ws.get(L.load().gw_scan_workspace_bytes(int(n) + 1))
+
+    def build_system(self):
+        """Row compaction and block-CSR pattern, once per load step."""
+        g, s = self.grid_struct(), self.stream
+        nr = C.c_int32(0)
+        L.call("gw_compact_rows", C.byref(g), _p(self.node_active), _p(self.boundary), _p(self.node2row),
+               _p(self.row2node), _p(self.free_mask), C.byref(nr), _p(self._scan_ws_for(self.n_nodes)), s)
+        self.n_rows = nr.value
+        if self._row_ptr.numel() < self.n_rows + 1:
+            self._row_ptr = torch.zeros(int((self.n_rows + 1) * 1.25) + 8, dtype=torch.int32, device=self.device)
+        nnzb = C.c_int32(0)
+        L.call("gw_pattern_count", C.byref(g), _p(self.cell_span), _p(self.node2row), _p(self.row2node),
+               self.n_rows, _p(self.stencil), _p(self._row_ptr), C.byref(nnzb),
+               _p(self._scan_ws_for(self.n_rows + 1)), s)
+        self.nnzb = nnzb.value
+        if self._cols.numel() < self.nnzb:
+            self._cols = torch.zeros(int(self.nnzb * 1.25) + 8, dtype=torch.int32, device=self.device)
+        vbytes = (8 if self.prec == L.PREC_F64 else 4) * self.nnzb * self.nf * self.nf
+        self._vals.get(vbytes)
+        b = self.bsr_struct()
+        L.call("gw_pattern_fill", C.byref(g), C.byref(b), _p(self._cols), s)
+        n = self.n_rows * self.nf
+        if self._R.numel() < n:
+            self._R = torch.zeros(int(n * 1.25) + 8, dtype=torch.float64, device=self.device)
+            self._delta = torch.zeros_like(self._R)
+
+    def project_pressure(self, cg_rtol=1e-13):
+        """Consistent-mass projection of particle pressure to the nodes (GPU CG)."""
+        g, pt, s = self.grid_struct(), self.particles_struct(), self.stream
+        self.touched.zero_()
+        L.call("gw_touched_nodes", C.byref(g), _p(self.cell_span), _p(self.touched), s)
+        nr = C.c_int32(0)
+        L.call("gw_compact_rows", C.byref(g), _p(self.touched), _p(self.boundary), _p(self.m_node2row),
+               _p(self.m_row2node), C.c_void_p(0), C.byref(nr), _p(self._scan_ws_for(self.n_nodes)), s)
+        self.m_rows = nr.value
+        if self._m_row_ptr.numel() < self.m_rows + 1:
+            self._m_row_ptr = torch.zeros(int((self.m_rows + 1) * 1.25) + 8, dtype=torch.int32, device=self.device)
+        nnzb = C.c_int32(0)
+        L.call("gw_pattern_count", C.byref(g), _p(self.cell_span), _p(self.m_node2row), _p(self.m_row2node),
+               self.m_rows, _p(self.m_stencil), _p(self._m_row_ptr), C.byref(nnzb),
+               _p(self._scan_ws_for(self.m_rows + 1)), s)
+        self.m_nnzb = nnzb.value
+        if self._m_cols.numel() < self.m_nnzb:
+            self._m_cols = torch.zeros(int(self.m_nnzb * 1.25) + 8, dtype=torch.int32, device=self.device)
+            self._m_vals = torch.zeros(int(self.m_nnzb * 1.25) + 8, dtype=torch.float64, device=self.device)
+        if self._m_rhs.numel() < self.m_rows:
+            self._m_rhs = torch.zeros(int(self.m_rows * 1.25) + 8, dtype=torch.float64, device=self.device)
+            self._m_x = torch.zeros_like(self._m_rhs)
+        M = self.bsr_struct(mass=True)
+        L.call("gw_pattern_fill", C.byref(g), C.byref(M), _p(self._m_cols), s)
+        st = self.step_struct(0, 1)
+        L.call("gw_mass_assemble", C.byref(g), C.byref(pt), _p(self.perm), C.byref(st), C.byref(M), _p(self._m_rhs), s)
+        self._m_x.zero_()
+        ws = self._kry_ws.get(L.load().gw_krylov_workspace_bytes(self.m_rows, 1, L.PREC_F64))
+        it, rr = C.c_int32(0), C.c_double(0.0)
+        rc = L.load().gw_bsr_krylov_solve(C.byref(M), L.PREC_F64, L.KRYLOV_CG, L.PRECOND_DIAG, _p(self._m_rhs),
+                                          _p(self._m_x), cg_rtol, 100000, _p(ws), C.byref(it), C.byref(rr), s)
+        if rc not in (L.GW_OK, L.GW_ENOCONV):
+            L.check(rc, "consistent-mass CG")
+        self.mass_cg_iters = it.value
+        L.call("gw_set_nodal_pressure", C.byref(g), _p(self.m_row2node), self.m_rows, _p(self._m_x), _p(self.boundary),
+               _p(self.node_active), _p(self.u_old), _p(self.u_new), s)
+
+    def step_struct(self, current_step, total_steps):
+        sp = self.step_params
+        st = L.Step()
+        st.current_step = float(current_step)
+        st.total_steps = float(total_steps)
+        st.gravity_mag = float(sp.get("gravity_mag", 0.0))
+        for k in range(3):
+            st.point_load[k] = float(sp.get("point_load", (0.0, 0.0, 0.0))[k])
+            st.traction[k] = float(sp.get("traction", (0.0, 0.0, 0.0))[k])
+        st.p_vol = float(sp["p_vol"])
+        st.p_rho = float(sp["p_rho"])
+        st.PPD = float(sp["PPD"])
+        st.dt = float(sp.get("dt", 0.0))
+        st.phi_initial = float(sp.get("phi_initial", 0.0))
+        st.mobility = float(sp.get("mobility", 0.0))
+        st.lp0 = float(sp["lp0"])
+        fo = sp.get("footing")
+        if fo is not None:
+            st.has_footing = 1
+            st.footing_min[0], st.footing_min[1] = fo["min"][0], fo["min"][1] if len(fo["min"]) > 1 else 0.0
+            st.footing_max[0], st.footing_max[1] = fo["max"][0], fo["max"][1] if len(fo["max"]) > 1 else 0.0
+            st.footing_initial_height = fo["initial_height"]
+            st.footing_incr_disp = fo["incr_disp"]
+            st.penalty_factor = fo["penalty_factor"]
+        return st
+
+    def assemble(self, mat_struct, current_step, total_steps, want_K=True):
+        g, pt, s = self.grid_struct(), self.particles_struct(), self.stream
+        st = self.step_struct(current_step, total_steps)
+        A = self.bsr_struct()
+        n = self.n_rows * self.nf
+        self.force.zero_()
+        self._R[:n].zero_()
+        L.call("gw_assemble", C.byref(g), C.byref(mat_struct), C.byref(st), C.byref(pt), _p(self.perm),
+               _p(self.free_mask), _p(self.u_new), _p(self.u_old), C.byref(A) if want_K else None, self.prec,
+               _p(self._R), _p(self.force), s)
+
+    def residual_norm_async(self):
+        n = self.n_rows * self.nf
+        L.call("gw_norm2", _p(self._R), n, _p(self.norm_dev), _p(self._norm_ws), self.stream)
+
+    def krylov(self, rtol=None):
+        A = self.bsr_struct()
+        n = self.n_rows * self.nf
+        self._delta[:n].zero_()
+        lib = L.load()
+        it, rr = C.c_int32(0), C.c_double(0.0)
+        rtol = rtol if rtol is not None else self.krylov_rtol
+        if self.krylov_method == "gmres":
+            ws = self._kry_ws.get(lib.gw_gmres_workspace_bytes(self.n_rows, self.nf, self.restart))
+            rc = lib.gw_bsr_gmres_solve(C.byref(A), self.prec, self.precond, _p(self._R), _p(self._delta), rtol,
+                                        self.krylov_max_iter, self.restart, _p(ws), C.byref(it), C.byref(rr),
+                                        self.stream)
+        else:
+            ws = self._kry_ws.get(lib.gw_krylov_workspace_bytes(self.n_rows, self.nf, self.prec))
+            rc = lib.gw_bsr_krylov_solve(C.byref(A), self.prec, L.KRYLOV_BICGSTAB, self.precond, _p(self._R),
+                                         _p(self._delta), rtol, self.krylov_max_iter, _p(ws), C.byref(it),
+                                         C.byref(rr), self.stream)
+        if rc not in (L.GW_OK, L.GW_ENOCONV, L.GW_EBREAKDOWN):
+            L.check(rc, "Krylov")
+        return it.value, rr.value, rc
+
+    def apply_increment(self):
+        A = self.bsr_struct()
+        L.call("gw_apply_increment", C.byref(A), _p(self._delta), _p(self.u_new), self.stream)
+
+    def g2p(self, current_step, total_steps):
+        g, pt = self.grid_struct(), self.particles_struct()
+        st = self.step_struct(current_step, total_steps)
+        L.call("gw_g2p", C.byref(g), C.byref(st), C.byref(pt), _p(self.u_new), _p(self.u_old), self.stream)
+
+    def device_status(self):
+        v = C.c_int32(0)
+        L.call("gw_read_device_status", C.byref(v), self.stream)
+        return v.value
+
+    # ------------------------------------------------------------------ Newton
+    def newton(self, mat_struct, current_step, total_steps, n_iter, tol):
+        """Newton loop with the reference's stopping rule
+        (solvers/quasi_static_solver_2d.py:151-231): R is assembled before the
+        update, the update is applied, then ||R|| < tol stops the loop."""
+        its = 0
+        for it in range(n_iter):
+            self.assemble(mat_struct, current_step, total_steps, want_K=True)
+            self.residual_norm_async()
+            kit, relres, rc = self.krylov()
+            self.apply_increment()
+            nrm = float(self.norm_dev.item())
+            its += 1
+            self.log.append((current_step, it, nrm, kit, relres, rc))
+            if not math.isfinite(nrm):
+                hist = "; ".join(f"it {l[1]}: |R|={l[2]:.3e} krylov {l[3]} relres {l[4]:.2e} rc {l[5]}"
+                                 for l in self.log[-its:])
+                raise L.GeoWarpError(L.GW_ENAN, "newton", f"non-finite residual norm at step {current_step} "
+                                     f"(device status {self.device_status()}; {hist})")
+            if nrm < tol:
+                break
+        return its
+
+    # ------------------------------------------------------------------ host views
+    def rows_to_field_major(self, vec_rows):
+        """Scatter an active-row vector to the reference's field-major layout."""
+        out = torch.zeros(self.nf * self.n_nodes, dtype=torch.float64, device=self.device)
+        nodes = self.row2node[: self.n_rows].long()
+        v = vec_rows[: self.n_rows * self.nf].view(self.n_rows, self.nf)
+        for f in range(self.nf):
+            out[f * self.n_nodes + nodes] = v[:, f]
+        return out
+
+    def node_to_field_major(self, u):
+        return u.view(self.n_nodes, self.nf).t().reshape(-1).contiguous()
+
+    def matrix_coo(self):
+        """Field-major COO triplets (rows, cols, vals) of the assembled K, for checks."""
+        nf, nr = self.nf, self.n_rows
+        rp = self._row_ptr[: nr + 1].long()
+        cols = self._cols[: self.nnzb].long()
+        counts = rp[1:] - rp[:-1]
+        brow = torch.repeat_interleave(torch.arange(nr, device=self.device), counts)
+        vt = torch.float64 if self.prec == L.PREC_F64 else torch.float32
+        vals = self._vals.t[: self.nnzb * nf * nf * (8 if vt == torch.float64 else 4)].view(vt).view(self.nnzb, nf, nf)
+        r2n = self.row2node[:nr].long()
+        rows_o, cols_o, vals_o = [], [], []
+        for f in range(nf):
+            for gcol in range(nf):
+                rows_o.append(f * self.n_nodes + r2n[brow])
+                cols_o.append(gcol * self.n_nodes + r2n[cols])
+                vals_o.append(vals[:, f, gcol].double())
+        return torch.cat(rows_o), torch.cat(cols_o), torch.cat(vals_o)

@@ -1,0 +1,273 @@
+/*
+ * geowarp_b200 — C ABI of the B200-native implicit cpGIMP engine.
+ *
+ * The reference (choo-group/GeoWarp) has no FFI: its boundary is the Python
+ * solver-class API (solvers/quasi_static_solver_2d.py:45-258,
+ * solvers/quasi_static_coupled_solver_2d.py:45-313,
+ * solvers/quasi_static_coupled_solver_3d.py:56-420) over Warp kernels in
+ * mpm/mpm_utils.py, mpm/gimp.py and solvers/sparse_differentiation.py.  Each
+ * entry point below replaces one of those Warp launches (or Warp/SciPy library
+ * calls) and is cited beside its declaration.  The Python solver classes in
+ * geowarp_b200/solvers bind these symbols through ctypes.
+ *
+ * Conventions
+ *  - All pointers are device pointers unless the name ends in _host.
+ *  - Memory is owned by the caller; no entry point allocates, except the
+ *    caller-sized workspaces passed in explicitly.
+ *  - Calls are ordered on the given stream and do not synchronise, except
+ *    gw_bsr_krylov_solve (which polls its residual on the host) and the
+ *    *_count entry points that return a size.
+ *  - Return value: 0 on success, a negative GW_E* code otherwise.
+ *  - Particle arrays are indexed by the user's particle id (the reference's
+ *    order).  Grid vectors are node-interleaved: value (node, field) at
+ *    node*nf + field.  Boundary flags are field-major like the reference's
+ *    boundary_flag_array: flag (field, node) at field*n_nodes + node.
+ */
+#ifndef GEOWARP_B200_H
+#define GEOWARP_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define GW_OK 0
+#define GW_EINVAL -1        /* bad sizes or null pointers                        */
+#define GW_ECUDA -2         /* a CUDA launch or API call failed                  */
+#define GW_ENOCONV -3       /* Krylov iteration cap reached before tolerance     */
+#define GW_EBREAKDOWN -4    /* Krylov breakdown (rho or omega underflow)         */
+#define GW_ENAN -5          /* non-finite value detected                         */
+#define GW_ERANGE -6        /* particle support left the grid                    */
+#define GW_EMODEL -7        /* unknown material model for this solver kind       */
+
+/* ------------------------------------------------------------ enums */
+#define GW_KIND_SOLID2D 0   /* quasi_static_solver_2d: unknowns (ux, uy)          */
+#define GW_KIND_COUPLED2D 1 /* quasi_static_coupled_solver_2d: (ux, uy, p)        */
+#define GW_KIND_COUPLED3D 2 /* quasi_static_coupled_solver_3d: (ux, uy, uz, p)    */
+
+#define GW_MODEL_HENCKY 0   /* 'Hencky elasticity' (mpm/mpm_utils.py:537-542)   */
+#define GW_MODEL_J2 1       /* 'J2' (materials/plasticity.py:8-37)                */
+#define GW_MODEL_NEOHOOKEAN 2 /* 'Neo-Hookean' (mpm/mpm_utils.py:914-916, 1204-1208) */
+#define GW_MODEL_LINEAR 3   /* small-strain linear elasticity (extension)         */
+#define GW_MODEL_DP 4       /* Drucker-Prager (triaxial_DruckerPrager.py:119-412) */
+#define GW_MODEL_NORSAND 5  /* NorSand (triaxial_NorSand.py:155-400)              */
+
+#define GW_PREC_F64 0       /* plain FP64 everywhere                               */
+#define GW_PREC_F32 1       /* FP32 values / FP32 accumulation                     */
+
+#define GW_PRECOND_DIAG 0   /* scalar Jacobi, the reference's ptype='diag'         */
+#define GW_PRECOND_BLOCK 1  /* node-block Jacobi (nf x nf inverse)                 */
+
+#define GW_KRYLOV_BICGSTAB 0
+#define GW_KRYLOV_CG 1
+#define GW_KRYLOV_GMRES 2
+
+/* ------------------------------------------------------------ structs */
+typedef struct gw_grid {
+    int32_t dim;            /* 2 or 3                                             */
+    int32_t kind;           /* GW_KIND_*                                          */
+    int32_t nf;             /* unknowns per node: 2, 3 or 4                       */
+    int32_t n_grid[3];      /* cells per axis (n_grid_z = 0 in 2D)                */
+    int32_t n_nodes;        /* prod(n_grid + 1)                                   */
+    int32_t pad0;
+    double h[3];            /* cell sizes seen by the shape functions (2D: dx,dx) */
+    double inv_h[3];
+    double h_nodes[3];      /* cell sizes for nodal positions (pressure BC)       */
+    double domain_min[3];   /* lp clipping box (mpm/gimp.py:449-459)              */
+    double domain_max[3];
+} gw_grid_t;
+
+typedef struct gw_material {
+    int32_t model;          /* GW_MODEL_*                                         */
+    int32_t dp_tension_cutoff; /* DP: 1 keeps the trial state when P_trial >= 0, as
+                                  the reference does (triaxial_DruckerPrager.py:347-349);
+                                  0 applies the cone return there too (extension) */
+    double youngs_modulus;  /* used when the per-particle E pointer is null       */
+    double poisson_ratio;
+    double kappa;           /* J2 yield radius                                    */
+    double friction_angle;  /* DP, degrees                                        */
+    double dilation_angle;  /* DP, degrees                                        */
+    double cohesion;        /* DP                                                 */
+    double shape_factor;    /* DP hyperbolic smoothing                            */
+    /* NorSand (triaxial_NorSand.py:13-43) */
+    double ns_kappa, ns_tilde_lambda, ns_M, ns_N, ns_beta, ns_vc0, ns_p0, ns_v0, ns_h;
+    double ns_shear_modulus, ns_eps_v0;
+} gw_material_t;
+
+typedef struct gw_step {
+    double current_step;    /* load ramp (step+1)/total_steps                     */
+    double total_steps;
+    double gravity_mag;
+    double point_load[3];
+    double traction[3];
+    double p_vol, p_rho, PPD;
+    double dt, phi_initial, mobility;   /* u-p only                               */
+    double lp0;             /* GIMP_lp_initial                                    */
+    int32_t has_footing;    /* penalty footing (mpm/mpm_utils.py:1234-1248)       */
+    int32_t pad0;
+    double footing_min[2], footing_max[2];
+    double footing_initial_height, footing_incr_disp, penalty_factor;
+} gw_step_t;
+
+/* Particle state, user order.  x, lp: [N*dim]; F*, b*, sigma: [N*9] row-major
+ * 3x3; pressure, pi_*: [N]; flags: uint8 [N]; E: [N] or NULL. */
+typedef struct gw_particles {
+    int32_t n;
+    int32_t pad0;
+    double *x, *x0, *lp;
+    double *F_old, *F_new, *b_old, *b_new, *sigma;
+    double *pressure, *pi_old, *pi_new;
+    const uint8_t *ext_flag, *trac_flag, *pbc_flag;
+    const double *E;
+} gw_particles_t;
+
+/* Block-CSR over active nodes.  Block (r, j) is nf x nf, row-major, at
+ * vals[(row_ptr[r] + j)*nf*nf].  cols[] are active-row indices. */
+typedef struct gw_bsr {
+    int32_t n_rows;
+    int32_t nf;
+    int32_t nnzb;
+    int32_t mask_words;     /* 1 (2D: 5x5 stencil) or 4 (3D: 5x5x5 stencil)       */
+    const int32_t *row_ptr; /* [n_rows+1]                                         */
+    const int32_t *cols;    /* [nnzb]                                             */
+    const int32_t *row2node;/* [n_rows]                                           */
+    const int32_t *node2row;/* [n_nodes], -1 for inactive nodes                   */
+    const uint32_t *stencil;/* [n_nodes*mask_words] coupled-offset bitmask        */
+    void *vals;             /* double or float per precision                      */
+} gw_bsr_t;
+
+/* ------------------------------------------------------------ queries */
+int gw_version(void);
+const char *gw_status_string(int code);
+/* Device-side error flag written by kernels (range / NaN); read & clear. */
+int gw_read_device_status(int32_t *flag_host, void *stream);
+
+/* ------------------------------------------------------------ cell sort
+ * Replaces nothing in the reference (which never reorders particles): the
+ * cell key is the lower-corner cell of mpm/gimp.py:33-36 and the sort is a
+ * stable LSD radix sort, so the order is a deterministic function of keys.
+ * keys_out[N], perm_out[N]: perm_out lists user particle ids by (cell, id).
+ * workspace: gw_sort_workspace_bytes(n) bytes. */
+int64_t gw_sort_workspace_bytes(int32_t n);
+int gw_cell_sort(const gw_grid_t *grid, const gw_particles_t *pt, int32_t *keys_out, int32_t *perm_out,
+                 void *workspace, void *stream);
+
+/* ------------------------------------------------------------ P2G activation
+ * Replaces P2G_2d (mpm/mpm_utils.py:83-136), the activation and pressure-BC
+ * parts of P2G_coupled_2d (:138-235) and P2G_coupled_3d (:259-352).
+ * node_active[n_nodes] (uint8) and cell_span[n_cells] (uint32 bitmask of
+ * per-axis 3-node spans | 0x80 occupied) are OR-accumulated: zero them first.
+ * boundary[nf*n_nodes] gets pressure Dirichlet flags for u-p kinds. */
+int gw_p2g_activate(const gw_grid_t *grid, const gw_particles_t *pt, const int32_t *perm, uint8_t *node_active,
+                    uint32_t *cell_span, uint8_t *boundary, void *stream);
+
+/* Nodes inside the span support of an occupied cell (touched[n_nodes], uint8;
+ * zero it first): the row set of the consistent-mass system, i.e. every node
+ * the reference's 81/729 mass triplets per particle can reach with a nonzero
+ * weight (mpm/mpm_utils.py:237-257, 354-383). */
+int gw_touched_nodes(const gw_grid_t *grid, const uint32_t *cell_span, uint8_t *touched, void *stream);
+
+/* Compact active nodes: node2row[n_nodes], row2node[n_nodes] (first n_rows
+ * valid), n_rows_host.  Also builds free_mask[n_nodes] (bit f set when DOF
+ * (node, f) is active and not a Dirichlet DOF).  Synchronises (returns a size). */
+int gw_compact_rows(const gw_grid_t *grid, const uint8_t *node_active, const uint8_t *boundary, int32_t *node2row,
+                    int32_t *row2node, uint8_t *free_mask, int32_t *n_rows_host, void *workspace, void *stream);
+int64_t gw_scan_workspace_bytes(int32_t n);
+
+/* ------------------------------------------------------------ pattern
+ * Replaces the fixed 25/125-slot COO layout of
+ * solvers/sparse_differentiation.py:213-401: builds, once per load step, the
+ * block-CSR pattern of node pairs that share a particle's support.
+ * stencil[n_nodes*mask_words]; row_ptr[n_rows+1]; nnzb_host; then
+ * gw_pattern_fill writes cols[nnzb]. */
+int gw_pattern_count(const gw_grid_t *grid, const uint32_t *cell_span, const int32_t *node2row, const int32_t *row2node,
+                     int32_t n_rows, uint32_t *stencil, int32_t *row_ptr, int32_t *nnzb_host, void *workspace,
+                     void *stream);
+int gw_pattern_fill(const gw_grid_t *grid, const gw_bsr_t *A, int32_t *cols, void *stream);
+
+/* ------------------------------------------------------------ consistent mass
+ * Replaces the consistent-mass triplets of P2G_coupled_2d (mpm_utils.py:237-257)
+ * and P2G_coupled_3d (:354-383) plus the host pyamg / Warp BiCGSTAB solve
+ * (solvers/quasi_static_coupled_solver_2d.py:287-300,
+ *  solvers/quasi_static_coupled_solver_3d.py:409-417): assembles the scalar
+ * block-CSR mass matrix M (same pattern, nf = 1, FP64) over all nodes touched
+ * by particle supports (mass_node2row) and rhs_b. */
+int gw_mass_assemble(const gw_grid_t *grid, const gw_particles_t *pt, const int32_t *perm, const gw_step_t *st,
+                     const gw_bsr_t *M, double *rhs, void *stream);
+/* Writes the projected nodal pressure into the p field of u_old and u_new for
+ * non-Dirichlet nodes (and, in 3D, active nodes): P2G_set_nodal_solution(_3d),
+ * mpm/mpm_utils.py:387-414. */
+int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_row2node, int32_t n_mass_rows, const double *p_hat,
+                          const uint8_t *boundary, const uint8_t *node_active, double *u_old, double *u_new,
+                          void *stream);
+
+/* ------------------------------------------------------------ residual + Jacobian
+ * Replaces assemble_residual_2d_hencky / _J2 (mpm/mpm_utils.py:416-780),
+ * assemble_residual_coupled_2d_neohookean (:782-1017),
+ * assemble_residual_coupled_3d_neohookean (:1020-1294) and the coloured
+ * reverse-AD Jacobian (solvers/quasi_static_solver_2d.py:169-198 and
+ * solvers/sparse_differentiation.py).  One thread per particle (cell order)
+ * evaluates the residual and, when A != NULL, its exact element tangent
+ * K = -dR/du, scattered element-by-element into A->vals (precision = prec).
+ * R_rows[n_rows*nf] (FP64) receives the masked residual; Dirichlet and
+ * inactive DOFs get identity rows (mpm/mpm_utils.py:1299-1341).
+ * force_host_accum: device double[1] accumulating the penalty footing force.
+ * Writes F_new, b_new, sigma, pi_new (state of this iterate). */
+int gw_assemble(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st, const gw_particles_t *pt,
+                const int32_t *perm, const uint8_t *free_mask, const double *u_new, const double *u_old,
+                const gw_bsr_t *A, int32_t prec, double *R_rows, double *force, void *stream);
+
+/* ------------------------------------------------------------ Krylov
+ * Replaces wp.optim.linear.bicgstab with the 'diag' preconditioner and the
+ * host spsolve / pyamg paths (solvers/quasi_static_solver_2d.py:236-256):
+ * hand-written BSR SpMV + fused dot/axpy kernels, FP64 inner products.
+ * Solves A x = b (x holds the initial guess).  rtol relative to ||b||.
+ * workspace: gw_krylov_workspace_bytes(n_rows, nf, prec) bytes.
+ * iters_host / relres_host receive the iteration count and final residual. */
+int64_t gw_krylov_workspace_bytes(int32_t n_rows, int32_t nf, int32_t prec);
+int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond, const double *b, double *x,
+                        double rtol, int32_t max_iter, void *workspace, int32_t *iters_host, double *relres_host,
+                        void *stream);
+/* Restarted right-preconditioned GMRES(restart), restart <= 128: the robust
+ * solver for the nonsymmetric, indefinite Jacobians (penalty footing, u-p
+ * saddle point) on which BiCGSTAB breaks down.  Classical Gram-Schmidt with
+ * one re-orthogonalisation; FP64 Krylov basis and inner products.
+ * workspace: gw_gmres_workspace_bytes(n_rows, nf, restart) bytes. */
+int64_t gw_gmres_workspace_bytes(int32_t n_rows, int32_t nf, int32_t restart);
+int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const double *b, double *x, double rtol,
+                       int32_t max_iter, int32_t restart, void *workspace, int32_t *iters_host, double *relres_host,
+                       void *stream);
+/* y = A x (x, y FP64 of length n_rows*nf; A values in prec). */
+int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream);
+/* y = A^T x. */
+int gw_bsr_spmv_t(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream);
+/* ||v||_2 of an FP64 vector into norm_dev[0] (device). */
+int gw_norm2(const double *v, int32_t n, double *norm_dev, void *workspace, void *stream);
+/* u_full[row2node[r]*nf+f] += delta[r*nf+f]: from_increment_to_solution
+ * (mpm/mpm_utils.py:1343-1348) restricted to the active rows. */
+int gw_apply_increment(const gw_bsr_t *A, const double *delta, double *u_full, void *stream);
+
+/* ------------------------------------------------------------ G2P
+ * Replaces G2P_2d / G2P_coupled_2d / G2P_coupled_3d (mpm/mpm_utils.py:1351-1590)
+ * fused with update_GIMP_lp_2d/3d (mpm/gimp.py:428-507): x += sum N du,
+ * F_old <- F_new, b_old <- b_new, pi_old <- pi_new, pressure = sum N p,
+ * lp update. */
+int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_particles_t *pt, const double *u_new,
+           const double *u_old, void *stream);
+
+/* ------------------------------------------------------------ single-point models
+ * Evaluates a return map for n independent principal trial strains (e_trial
+ * [n*3]) — the material tests of problems/material_tests/triaxial_*.py.
+ * e_out[n*3]; tau_out[n*3] principal Kirchhoff; dtau_de_out[n*9] (may be NULL)
+ * the algorithmic tangent d tau_A / d e_trial_B; eps_v_total[n] and pi_old,
+ * pi_new (NorSand state) may be NULL for other models. */
+int gw_return_map(const gw_material_t *mat, int32_t n, const double *e_trial, const double *eps_v_total,
+                  const double *pi_old, double *pi_new, double *e_out, double *tau_out, double *dtau_de_out,
+                  void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GEOWARP_B200_H */

@@ -1,0 +1,131 @@
+"""CPU checks of the oracle: analytic known answers from the reference's own
+driver scripts, exactness of its complex-step tangents, and the committed
+golden fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+import cases
+from oracle.eig import eigh3
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def golden(name):
+    return dict(np.load(os.path.join(GOLDEN, name + ".npz")))
+
+
+@pytest.mark.parametrize("material", ["Hencky elasticity", "J2"])
+def test_bar_self_weight_known_answer(material):
+    """Relative L1 error of sigma_yy against rho g (H - (y0 - start_y)), the
+    check of problems/bar_compaction_J2/bar_compaction_cpGIMP_J2.py:113-131."""
+    H = 12.5
+    grid, parts, it, mat, load = cases.bar_dicts(material, height=H)
+    o = cases.oracle_solid2d(grid, parts, it, mat, load)
+    cases.bar_boundary(o.boundary, grid["n_grid_x"], grid["n_grid_y"])
+    n_steps = 10
+    for k in range(n_steps):
+        o.advance_one_step(k, n_steps)
+    rho, g = parts["p_rho"], load["gravity_mag"]
+    ana = rho * (-g) * (H - (o.x0[:, 1] - grid["start_y"]))
+    err = np.abs(o.sigma[:, 1, 1] - ana).sum() / (g * rho * H * o.N)
+    assert err < 5e-3, err
+    assert max(o.iters) <= 6  # quadratic Newton convergence with the exact tangent
+
+
+def test_oracle_reproduces_golden_bar():
+    g = golden("bar_hencky")
+    grid, parts, it, mat, load = cases.bar_dicts("Hencky elasticity", height=12.5)
+    o = cases.oracle_solid2d(grid, parts, it, mat, load)
+    cases.bar_boundary(o.boundary, grid["n_grid_x"], grid["n_grid_y"])
+    steps, n_steps = g["steps"]
+    for k in range(steps):
+        o.advance_one_step(k, n_steps)
+    assert np.array_equal(o.active, g["active"])
+    assert np.abs(o.x - g["x"]).max() < 1e-13
+    assert np.abs(o.sigma - g["sigma"]).max() < 1e-11 * np.abs(g["sigma"]).max()
+
+
+def test_oracle_reproduces_golden_terzaghi():
+    g = golden("terzaghi")
+    grid, parts, it, mat, porous, load = cases.terzaghi_dicts(n_cells_y=12)
+    o = cases.oracle_coupled2d(grid, parts, it, mat, porous, load)
+    top = cases.top_flags(o.x, grid["end_y"], grid["dx"], parts["PPD"])
+    o.pbc_flag[:] = top
+    o.trac_flag[:] = top
+    for k in range(4):
+        o.advance_one_step(k, 600, set_boundary=lambda b: cases.terzaghi_boundary_np(b, grid["n_grid_x"], grid["n_grid_y"]))
+    assert np.array_equal(o.boundary, g["boundary"])
+    assert np.abs(o.pressure - g["pressure"]).max() < 1e-11 * np.abs(g["pressure"]).max()
+
+
+def _fd_check(o, step, n_steps, rng, h=1e-7):
+    R, K, _ = o.assemble(step, n_steps)
+    free = o.active & ~o.boundary
+    v = np.where(free, rng.normal(size=o.ndof), 0.0)
+    u0 = o.u_new.copy()
+    o.u_new = u0 + h * v
+    Rp, _, _ = o.assemble(step, n_steps, want_K=False)
+    o.u_new = u0 - h * v
+    Rm, _, _ = o.assemble(step, n_steps, want_K=False)
+    o.u_new = u0
+    fd = -(Rp - Rm) / (2 * h)
+    Kv = K @ v
+    return np.abs(Kv[free] - fd[free]).max() / np.abs(fd[free]).max()
+
+
+def test_oracle_tangent_matches_fd_solid():
+    rng = np.random.default_rng(0)
+    grid, parts, it, mat, load = cases.bar_dicts("J2", height=6.25)
+    o = cases.oracle_solid2d(grid, parts, it, mat, load)
+    cases.bar_boundary(o.boundary, grid["n_grid_x"], grid["n_grid_y"])
+    o.advance_one_step(0, 4)
+    o.u_new[:] = 0.0
+    o.p2g()
+    assert _fd_check(o, 1, 4, rng) < 1e-6
+
+
+def test_oracle_tangent_matches_fd_footing():
+    rng = np.random.default_rng(1)
+    grid, parts, it, mat, load = cases.footing_dicts(nx=8, ny=4, n_steps=10)
+    o = cases.oracle_solid2d(grid, parts, it, mat, load)
+    cases.footing_boundary(o.boundary, grid)
+    o.p2g()
+    o.u_new = rng.normal(scale=1e-4, size=o.ndof) * (o.active & ~o.boundary)
+    assert _fd_check(o, 0, 10, rng, h=1e-9) < 1e-5
+
+
+def test_oracle_tangent_matches_fd_coupled():
+    rng = np.random.default_rng(2)
+    grid, parts, it, mat, porous, load = cases.terzaghi_dicts(n_cells_y=6)
+    o = cases.oracle_coupled2d(grid, parts, it, mat, porous, load)
+    top = cases.top_flags(o.x, grid["end_y"], grid["dx"], parts["PPD"])
+    o.pbc_flag[:] = top
+    o.trac_flag[:] = top
+    cases.terzaghi_boundary_np(o.boundary, grid["n_grid_x"], grid["n_grid_y"])
+    o.p2g()
+    o.u_new = o.u_new + rng.normal(scale=1e-3, size=o.ndof) * (o.active & ~o.boundary)
+    assert _fd_check(o, 0, 600, rng, h=1e-8) < 1e-5
+
+
+def test_eigh3_reconstruction_and_complex_step():
+    rng = np.random.default_rng(3)
+    A = rng.normal(size=(64, 3, 3))
+    A = A + A.transpose(0, 2, 1)
+    lam, V = eigh3(A)
+    assert np.abs(np.einsum("nia,na,nja->nij", V, lam, V) - A).max() < 1e-13
+    E = rng.normal(size=(64, 3, 3))
+    E = E + E.transpose(0, 2, 1)
+    lc, Vc = eigh3(A + 1e-30j * E)
+    dl = np.imag(lc) / 1e-30
+    ana = np.einsum("nia,nij,nja->na", V, E, V)  # dlambda_a = v_a^T E v_a
+    assert np.abs(dl - ana).max() < 1e-12
+
+
+def test_triaxial_dp_reaches_the_cone():
+    g = golden("triaxial_dp")
+    phi = np.deg2rad(35.0)
+    M = 6 * np.sin(phi) / (3 - np.sin(phi))
+    assert abs(g["Q"][-1] / g["P"][-1] - M) < 2e-3 * M
+    assert np.all(np.diff(g["Q"][:4]) > 0)
