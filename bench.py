@@ -1,0 +1,294 @@
+"""Benchmark: load steps/s of the implicit cpGIMP engine on the plane-strain
+Drucker-Prager strip footing (256 x 128 soil cells, 2 x 2 particles per cell
+= 131,072 particles, 1 m footing pushed 0.2 m over 100 load steps).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geowarp|reference]
+
+One "step" is one load step: P2G (cell sort, activation, pattern), the Newton
+loop (residual + exact element tangent, GMRES on the block-CSR Jacobian) and
+G2P, followed by its adjoint (transpose solve with the converged Jacobian and
+the adjoint P2G/G2P), in the mixed FP32/FP64 mode.  The plain FP64 engine runs
+the same steps for the error check and is reported beside it.  With N GPUs
+the job runs N independent replicas (one per rank; there is no data-path
+collective) and `value` is the aggregate over ranks.
+
+--impl reference times the CPU restatement of the reference's algorithm (the
+reference itself runs only on NVIDIA Warp, not installable here) on a bounded
+sample of the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "load steps/s (fwd+adjoint), mixed vs plain FP64 on same B200 at rel err<=1e-6"
+WORKLOAD = dict(workload="2D plane-strain rigid strip footing on Drucker-Prager soil",
+                cells="256x128 soil cells (260x132 grid), dx=0.05 m", particles=131072, ppc="2x2",
+                material="DP E=2e7 Pa nu=0.3 c=10 kPa phi=30 psi=0", footing="1 m wide, 0.2 m over 100 steps")
+N_STEPS_TOTAL = 100
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="geowarp", choices=["geowarp", "reference"])
+    ap.add_argument("--small", action="store_true", help="64x32-cell variant for quick checks")
+    ap.add_argument("--profile", action="store_true", help="also time the dominant kernel (instrumented pass)")
+    return ap.parse_args()
+
+
+def footing_kwargs(small):
+    return dict(n_cells_x=64, n_cells_y=32, footing_width=0.25) if small else {}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+
+    def __enter__(self):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [l.split(",") for l in open(self.f.name).read().strip().split("\n") if l.strip()]
+        except OSError:
+            rows = []
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for name, v in zip(names, r[5:9]):
+                if v.strip() == "Active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_geowarp(args):
+    import torch
+    import torch.distributed as dist
+    from geowarp_b200 import problems
+    from geowarp_b200.adjoint import LoadStepAdjoint
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    dev = torch.device("cuda", torch.cuda.current_device())
+    fk = footing_kwargs(args.small)
+    W, K = args.warmup, args.steps
+
+    def sync():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            dist.barrier()
+
+    def one_step(s, adj, k):
+        # forward load step (checkpointed), then its adjoint seeded with the
+        # displacement misfit of L = 1/2 |x - x0|^2
+        adj.forward_step(k, N_STEPS_TOTAL, keep=False)
+        adj.seed_displacement_misfit()
+        adj.backward_step()
+
+    # ---- mixed precision, resident (value)
+    s_mx = problems.strip_footing_2d(precision="mixed", device=dev, **fk)
+    adj_mx = LoadStepAdjoint(s_mx)
+    for k in range(W):
+        one_step(s_mx, adj_mx, k)
+    sync()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as cs:
+        sync()
+        ev0.record()
+        for k in range(W, W + K):
+            one_step(s_mx, adj_mx, k)
+        ev1.record()
+        sync()
+    ms_mx = ev0.elapsed_time(ev1)
+    clocks = cs.summary()
+
+    # ---- plain FP64 on the same steps (error reference and its own throughput)
+    s_64 = problems.strip_footing_2d(precision="fp64", device=dev, **fk)
+    adj_64 = LoadStepAdjoint(s_64)
+    for k in range(W):
+        one_step(s_64, adj_64, k)
+    sync()
+    ev0.record()
+    for k in range(W, W + K):
+        one_step(s_64, adj_64, k)
+    ev1.record()
+    sync()
+    ms_64 = ev0.elapsed_time(ev1)
+    disp_mx = (s_mx.x_particles - s_mx.x0)
+    disp_64 = (s_64.x_particles - s_64.x0)
+    rel_disp = float((disp_mx - disp_64).abs().max() / disp_64.abs().max())
+    rel_sig = float((s_mx.particle_Cauchy_stress_array - s_64.particle_Cauchy_stress_array).abs().max()
+                    / s_64.particle_Cauchy_stress_array.abs().max())
+    rel_grad = float((adj_mx.grad_E - adj_64.grad_E).abs().max() / adj_64.grad_E.abs().max().clamp_min(1e-300))
+
+    # ---- end to end through the public API with host-resident state
+    s_e2e = problems.strip_footing_2d(precision="mixed", device=dev, **fk)
+    adj_e2e = LoadStepAdjoint(s_e2e)
+    e = s_e2e.engine
+    host = {name: torch.empty_like(getattr(e, name), device="cpu").pin_memory()
+            for name in ("x", "F_old", "b_old", "lp", "pi_old")}
+    out_host = {name: torch.empty_like(getattr(e, name), device="cpu").pin_memory() for name in ("x", "sigma")}
+    for name in host:
+        host[name].copy_(getattr(e, name))
+    grad_host = torch.empty(e.N, dtype=torch.float64).pin_memory()
+    for k in range(W):
+        one_step(s_e2e, adj_e2e, k)
+    for name in host:
+        host[name].copy_(getattr(e, name))
+    sync()
+    h2d = sum(t.numel() * t.element_size() for t in host.values())
+    d2h = sum(t.numel() * t.element_size() for t in out_host.values()) + grad_host.numel() * 8
+    ev0.record()
+    for k in range(W, W + K):
+        for name, t in host.items():
+            getattr(e, name).copy_(t, non_blocking=True)
+        one_step(s_e2e, adj_e2e, k)
+        for name, t in out_host.items():
+            t.copy_(getattr(e, name), non_blocking=True)
+        grad_host.copy_(adj_e2e.grad_E, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        for name in host:
+            host[name].copy_(getattr(e, name))  # the host keeps the evolving state
+    ev1.record()
+    sync()
+    ms_e2e = ev0.elapsed_time(ev1)
+
+    # ---- dominant kernel, instrumented pass (not part of value)
+    roof = roofline_pass(s_mx, adj_mx, W + K, fk, dev) if args.profile or True else None
+
+    vals = torch.tensor([ms_mx, ms_64, ms_e2e], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    ms_mx, ms_64, ms_e2e = vals.tolist()
+    if rank == 0:
+        steps_total = K * world
+        line = {
+            "metric": METRIC, "value": steps_total / (ms_mx / 1e3), "unit": "load steps/s", "n_gpus": world,
+            "steps": K, "warmup": W, "ms_per_step": ms_mx / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
+            "config": dict(WORKLOAD, parallelism=f"replicas x{world}", global_batch=world, seq_len=None,
+                           l2="inputs larger than L2 not required: steps advance the state; no cached outputs",
+                           small=bool(args.small)),
+            "plain_fp64": {"value": steps_total / (ms_64 / 1e3), "ms_per_step": ms_64 / K},
+            "mixed_over_fp64": ms_64 / ms_mx,
+            "rel_err_vs_fp64": {"displacement": rel_disp, "cauchy_stress": rel_sig, "grad_E": rel_grad},
+            "e2e": {"value": steps_total / (ms_e2e / 1e3), "unit": "load steps/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": None,
+            "newton": {"mixed_iters": newton_stats(s_mx.engine), "fp64_iters": newton_stats(s_64.engine)},
+            "roofline": roof,
+            "clocks": clocks,
+        }
+        line["cpu_baseline"] = cpu_baseline(fk, line)
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def newton_stats(engine):
+    steps = {}
+    kry = []
+    for (step, it, nrm, kit, relres, rc) in engine.log:
+        steps[step] = steps.get(step, 0) + 1
+        kry.append(kit)
+    return {"mean_newton_per_step": float(np.mean(list(steps.values()))) if steps else None,
+            "mean_krylov_per_newton": float(np.mean(kry)) if kry else None}
+
+
+def roofline_pass(s, adj, k, fk, dev):
+    """Time the dominant kernel family with CUDA events inside one more step."""
+    import json as _json
+    from geowarp_b200 import profiling
+    peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    with profiling.kernel_timer() as kt:
+        adj.forward_step(k, N_STEPS_TOTAL, keep=False)
+        adj.seed_displacement_misfit()
+        adj.backward_step()
+    return profiling.roofline_summary(kt, peaks, peak_kind="measured" if "when" in peaks else "fallback")
+
+
+def cpu_baseline(fk, gpu_line):
+    """Oracle (CPU restatement) timing on a bounded sample, run on rank 0."""
+    from oracle.bench_sample import oracle_newton_sample
+    sec_per_newton, sample = oracle_newton_sample()
+    its = gpu_line["newton"]["fp64_iters"]["mean_newton_per_step"] or 1.0
+    return {"value": 1.0 / (sec_per_newton * its), "unit": "load steps/s", "cores": 1, "kind": "port",
+            "sample": sample + f"; scaled by {its:.2f} Newton iterations per load step (forward only)"}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle.bench_sample import oracle_newton_sample
+    times = []
+    for _ in range(max(1, min(args.steps, 2))):
+        sec, sample = oracle_newton_sample()
+        times.append(sec)
+    sec = float(np.median(times))
+    its = 8.0
+    v = 1.0 / (sec * its)
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "load steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "config": WORKLOAD,
+        "cpu_baseline": {"value": v, "unit": "load steps/s", "cores": 1, "kind": "port",
+                         "sample": sample + f"; scaled by an assumed {its} Newton iterations per load step"},
+        "e2e": {"value": v, "unit": "load steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_geowarp(a)

@@ -47,7 +47,7 @@ class Step(C.Structure):
                 ("point_load", C.c_double * 3), ("traction", C.c_double * 3),
                 ("p_vol", C.c_double), ("p_rho", C.c_double), ("PPD", C.c_double),
                 ("dt", C.c_double), ("phi_initial", C.c_double), ("mobility", C.c_double), ("lp0", C.c_double),
-                ("has_footing", C.c_int32), ("pad0", C.c_int32),
+                ("has_footing", C.c_int32), ("footing_stable", C.c_int32),
                 ("footing_min", C.c_double * 2), ("footing_max", C.c_double * 2),
                 ("footing_initial_height", C.c_double), ("footing_incr_disp", C.c_double),
                 ("penalty_factor", C.c_double)]
@@ -65,6 +65,10 @@ class Bsr(C.Structure):
     _fields_ = [("n_rows", C.c_int32), ("nf", C.c_int32), ("nnzb", C.c_int32), ("mask_words", C.c_int32),
                 ("row_ptr", C.c_void_p), ("cols", C.c_void_p), ("row2node", C.c_void_p), ("node2row", C.c_void_p),
                 ("stencil", C.c_void_p), ("vals", C.c_void_p)]
+
+
+class Adjoint(C.Structure):
+    _fields_ = [("x", C.c_void_p), ("lp", C.c_void_p), ("F", C.c_void_p), ("b", C.c_void_p), ("E", C.c_void_p)]
 
 
 P = C.c_void_p
@@ -100,6 +104,15 @@ SIGNATURES = {
     "gw_apply_increment": (C.c_int, [C.POINTER(Bsr), P, P, P]),
     "gw_g2p": (C.c_int, [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Particles), P, P, P]),
     "gw_return_map": (C.c_int, [C.POINTER(Material), I32, P, P, P, P, P, P, P, P]),
+    "gw_profile_enable": (C.c_int, [I32]),
+    "gw_profile_reset": (C.c_int, []),
+    "gw_profile_read": (C.c_int, [I32, PD, C.POINTER(C.c_int64), PD]),
+    "gw_profile_name": (C.c_char_p, [I32]),
+    "gw_bsr_transpose": (C.c_int, [C.POINTER(Grid), C.POINTER(Bsr), I32, P, P]),
+    "gw_adjoint_g2p": (C.c_int, [C.POINTER(Grid), C.POINTER(Material), C.POINTER(Step), C.POINTER(Particles), P, P,
+                                 P, C.POINTER(Bsr), C.POINTER(Adjoint), C.POINTER(Adjoint), P, P]),
+    "gw_adjoint_residual": (C.c_int, [C.POINTER(Grid), C.POINTER(Material), C.POINTER(Step), C.POINTER(Particles),
+                                      P, P, P, C.POINTER(Bsr), P, C.POINTER(Adjoint), P]),
 }
 
 _lib = None

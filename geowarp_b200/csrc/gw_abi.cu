@@ -6,6 +6,7 @@
 
 #include "gw_step_kernels.cuh"
 #include "gw_krylov.cuh"
+#include "gw_adjoint.cuh"
 
 using namespace gw;
 
@@ -31,6 +32,44 @@ thread_local char g_msg[512];
     } while (0)
 
 inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+
+// -------------------------------------------------------------- optional kernel timing
+// When enabled, selected launches are bracketed by CUDA events on their stream;
+// gw_profile_read() synchronises and reports per-class totals and the
+// algorithmic bytes the host attributed to each launch.
+enum ProfClass { PC_ASSEMBLE = 0, PC_SPMV, PC_DOTS, PC_UPDATE, PC_NEXT, PC_G2P, PC_ADJ_G2P, PC_ADJ_RES, PC_COUNT };
+const char *kProfNames[PC_COUNT] = {"k_assemble", "k_gm_spmv", "k_gm_dots", "k_gm_update", "k_gm_next", "k_g2p",
+                                    "k_adjoint_g2p", "k_adjoint_residual"};
+struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
+bool g_prof_on = false;
+ProfRec *g_prof = nullptr;
+int g_prof_n = 0, g_prof_cap = 0;
+double g_prof_ms[PC_COUNT], g_prof_bytes[PC_COUNT];
+long g_prof_count[PC_COUNT];
+
+struct ProfScope {
+    ProfRec *r = nullptr;
+    cudaStream_t s;
+    ProfScope(int cls, cudaStream_t st, double bytes) : s(st) {
+        if (!g_prof_on) return;
+        if (g_prof_n == g_prof_cap) {
+            int nc = g_prof_cap ? 2 * g_prof_cap : 4096;
+            ProfRec *nr = (ProfRec *)realloc(g_prof, sizeof(ProfRec) * nc);
+            if (!nr) return;
+            g_prof = nr;
+            g_prof_cap = nc;
+        }
+        r = &g_prof[g_prof_n++];
+        r->cls = cls;
+        r->bytes = bytes;
+        cudaEventCreate(&r->a);
+        cudaEventCreate(&r->b);
+        cudaEventRecord(r->a, s);
+    }
+    ~ProfScope() {
+        if (r) cudaEventRecord(r->b, s);
+    }
+};
 inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 inline int red_grid_rows(int n_rows) { int b = nblk(n_rows, kThreads / 32); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
 inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
@@ -298,6 +337,13 @@ int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const
                     cudaStream_t s) {
     const int b = nblk(p.n, kThreads);
     if (p.n > 0) {
+        const int D = KindTraits<KIND>::D, NF = KindTraits<KIND>::NF, NS = KindTraits<KIND>::NS;
+        // algorithmic bytes: particle state in (x, lp, F_old, b_old, E), state out
+        // (F_new, b_new, sigma), nodal gather (2 x NS x NF doubles), residual and
+        // the element blocks scattered into the matrix (span^D x span^D blocks)
+        const double per_p = 8.0 * (2 * D + 9 + 9 + 1) + 8.0 * 27 + 8.0 * 2 * NS * NF + 8.0 * NS * NF;
+        const double mat = A ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
+        ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + mat);
         if (!A) k_assemble<KIND, false, double><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         else if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         else k_assemble<KIND, true, float><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
@@ -471,14 +517,17 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
         GW_CUDA(cudaStreamSynchronize(s));
         if (h.done) break;
         int chunk = 4;
+        int kk = 0;  // host-side column estimate (exact until the cycle closes early)
+        const double spmv_bytes = (double)A->nnzb * (NF * NF * sizeof(VT) + 4) + 4.0 * (nr + 1) + 16.0 * n;
         for (;;) {
-            for (int it = 0; it < chunk; ++it) {
-                k_gm_spmv<NF, VT><<<gr, kThreads, 0, s>>>(a, G);
-                k_gm_dots<<<gv, kThreads, 0, s>>>(G, 0);
-                k_gm_update<<<gv, kThreads, 0, s>>>(G, 0);
-                k_gm_dots<<<gv, kThreads, 0, s>>>(G, 1);
-                k_gm_update<<<gv, kThreads, 0, s>>>(G, 1);
-                k_gm_next<NF><<<ge, kThreads, 0, s>>>(nr, G, 0);
+            for (int it = 0; it < chunk; ++it, ++kk) {
+                const double vb = 8.0 * n * (kk + 2);
+                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv<NF, VT><<<gr, kThreads, 0, s>>>(a, G); }
+                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gv, kThreads, 0, s>>>(G, 0); }
+                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gv, kThreads, 0, s>>>(G, 0); }
+                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gv, kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gv, kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_NEXT, s, 8.0 * n * 3 + 8.0 * nr * NF * NF); k_gm_next<NF><<<ge, kThreads, 0, s>>>(nr, G, 0); }
             }
             GW_LAUNCHED();
             GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
@@ -608,6 +657,8 @@ extern "C" int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_parti
     LaunchConst c = make_lc(grid, nullptr, st);
     PtrsP p = make_ptrs(*pt);
     const int b = nblk(pt->n, kThreads);
+    ProfScope ps(PC_G2P, S(stream), (double)pt->n * 8.0 * (2 * grid->dim * 3 + 9 * 4 + 3) +
+                                        (double)pt->n * 27.0 * 8.0 * grid->nf * 2);
     switch (grid->kind) {
         case GW_KIND_SOLID2D: k_g2p<GW_KIND_SOLID2D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
         case GW_KIND_COUPLED2D: k_g2p<GW_KIND_COUPLED2D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
@@ -632,3 +683,101 @@ extern "C" int gw_return_map(const gw_material_t *mat, int32_t n, const double *
     GW_LAUNCHED();
     return GW_OK;
 }
+
+// ==================================================================== adjoint (2D solid)
+namespace {
+AdjState make_adj(const gw_adjoint_t &a) {
+    AdjState s;
+    s.x = a.x; s.lp = a.lp; s.F = a.F; s.b = a.b; s.E = a.E;
+    return s;
+}
+}  // namespace
+
+extern "C" int gw_bsr_transpose(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, void *AT_vals, void *stream) {
+    GW_REQUIRE(grid && A && AT_vals);
+    if (A->n_rows == 0) return GW_OK;
+    PtrsA a = make_ptrs(*A);
+    cudaStream_t s = S(stream);
+    const size_t vb = (prec == GW_PREC_F64 ? 8 : 4) * (size_t)A->nnzb * A->nf * A->nf;
+    GW_CUDA(cudaMemsetAsync(AT_vals, 0, vb, s));
+    const int b = nblk(A->n_rows, kThreads / 32);
+    if (grid->dim == 2) {
+        if (prec == GW_PREC_F64) k_bsr_transpose<2, double><<<b, kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
+        else k_bsr_transpose<2, float><<<b, kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
+    } else {
+        if (prec == GW_PREC_F64) k_bsr_transpose<3, double><<<b, kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
+        else k_bsr_transpose<3, float><<<b, kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
+    }
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+extern "C" int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
+                              const gw_particles_t *pt, const double *u_new, const double *u_old,
+                              const uint8_t *free_mask, const gw_bsr_t *A, const gw_adjoint_t *seed_in,
+                              gw_adjoint_t *q_out, double *ubar_rows, void *stream) {
+    GW_REQUIRE(grid && mat && st && pt && u_new && u_old && free_mask && A && seed_in && q_out && ubar_rows);
+    if (grid->kind != GW_KIND_SOLID2D) return GW_EMODEL;
+    if (mat->model == GW_MODEL_NORSAND) return GW_EMODEL;
+    cudaStream_t s = S(stream);
+    GW_CUDA(cudaMemsetAsync(ubar_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
+    if (pt->n == 0) return GW_OK;
+    LaunchConst c = make_lc(grid, mat, st);
+    ProfScope ps(PC_ADJ_G2P, s, (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 18 + 23 + 2 * 9 * 2));
+    k_adjoint_g2p<<<nblk(pt->n, 128), 128, 0, s>>>(c, make_ptrs(*pt), u_new, u_old, free_mask, make_ptrs(*A),
+                                                 make_adj(*seed_in), make_adj(*q_out), ubar_rows);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
+                                   const gw_particles_t *pt, const double *u_new, const double *u_old,
+                                   const uint8_t *free_mask, const gw_bsr_t *A, const double *lambda_rows,
+                                   gw_adjoint_t *q_out, void *stream) {
+    GW_REQUIRE(grid && mat && st && pt && u_new && u_old && free_mask && A && lambda_rows && q_out);
+    if (grid->kind != GW_KIND_SOLID2D) return GW_EMODEL;
+    if (mat->model == GW_MODEL_NORSAND) return GW_EMODEL;
+    if (pt->n == 0) return GW_OK;
+    LaunchConst c = make_lc(grid, mat, st);
+    ProfScope ps(PC_ADJ_RES, S(stream), (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 23 * 2 + 2 * 9 * 2 + 9 * 2));
+    k_adjoint_residual<<<nblk(pt->n, 128), 128, 0, S(stream)>>>(c, make_ptrs(*pt), u_new, u_old, free_mask,
+                                                                make_ptrs(*A), lambda_rows, make_adj(*q_out));
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
+// ==================================================================== kernel timing
+extern "C" int gw_profile_enable(int32_t on) {
+    g_prof_on = on != 0;
+    return GW_OK;
+}
+
+extern "C" int gw_profile_read(int32_t cls, double *ms_total_host, int64_t *launches_host, double *bytes_host) {
+    GW_REQUIRE(ms_total_host && launches_host && bytes_host && cls >= 0 && cls < PC_COUNT);
+    // fold pending records
+    for (int i = 0; i < g_prof_n; ++i) {
+        ProfRec &r = g_prof[i];
+        GW_CUDA(cudaEventSynchronize(r.b));
+        float ms = 0.f;
+        GW_CUDA(cudaEventElapsedTime(&ms, r.a, r.b));
+        g_prof_ms[r.cls] += ms;
+        g_prof_bytes[r.cls] += r.bytes;
+        g_prof_count[r.cls] += 1;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof_n = 0;
+    *ms_total_host = g_prof_ms[cls];
+    *launches_host = g_prof_count[cls];
+    *bytes_host = g_prof_bytes[cls];
+    return GW_OK;
+}
+
+extern "C" int gw_profile_reset(void) {
+    for (int i = 0; i < g_prof_n; ++i) { cudaEventDestroy(g_prof[i].a); cudaEventDestroy(g_prof[i].b); }
+    g_prof_n = 0;
+    for (int c = 0; c < PC_COUNT; ++c) { g_prof_ms[c] = 0.0; g_prof_bytes[c] = 0.0; g_prof_count[c] = 0; }
+    return GW_OK;
+}
+
+extern "C" const char *gw_profile_name(int32_t cls) { return (cls >= 0 && cls < PC_COUNT) ? kProfNames[cls] : ""; }

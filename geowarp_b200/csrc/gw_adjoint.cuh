@@ -1,0 +1,411 @@
+// Adjoint of one 2D solid load step (vector-Jacobian products per particle).
+//
+// The reference differentiates only the last residual with its Warp tape
+// (solvers/quasi_static_coupled_solver_3d.py:323-325).  The engine's adjoint is
+// the total derivative of a load step: with u* solving R(u; q) = 0 for the
+// particle inputs q = (x, lp, F_old, b_old, E),
+//   q_bar = d(out)/dq^T out_bar + R_q^T lambda,   K^T lambda = d(out)/du^T out_bar,
+// where out = (x_new, lp_new, F_new, b_new) are the G2P outputs
+// (mpm/mpm_utils.py:1351-1419, mpm/gimp.py:428-462) and K = -dR/du the
+// converged Jacobian.  Both VJPs come from one forward-mode pass per particle
+// with 19 dual lanes through the same formulas as the forward kernels:
+//   lanes 0-1 x, 2-3 lp, 4-8 F_old (00,01,10,11,22), 9-12 b_old (00,01=10,11,22),
+//   13 E, 14-17 H (00,01,10,11), 18 ubar_y (penalty footing).
+#pragma once
+#include "gw_step_kernels.cuh"
+
+namespace gw {
+
+constexpr int kAdjLanes = 19;
+typedef Dual<kAdjLanes, double> AD;
+constexpr int LX = 0, LLP = 2, LF = 4, LB = 9, LE = 13, LH = 14, LU = 18;
+
+GW_HD AD seed(double v, int lane) {
+    AD r(v);
+    if (lane >= 0) r.d[lane] = 1.0;
+    return r;
+}
+
+// cpGIMP axis with dual position and half-width; the cell indices come from
+// the values (piecewise-constant), the weights carry the lanes.
+GW_HD void gimp_axis_dual(const AD &xp, const AD &lp, double d, double inv_d, int &lower, int &span, AD w[3],
+                          AD g[3]) {
+    lower = cell_of(xp.v - lp.v, inv_d);
+    const int upper = cell_of(xp.v + lp.v, inv_d);
+    const int base = cell_of(xp.v, inv_d);
+    if (upper == lower) {
+        span = 2;
+        AD fx = xp * inv_d - (double)base;
+        w[0] = 1.0 - fx; w[1] = fx; w[2] = AD(0.0);
+        g[0] = AD(-inv_d); g[1] = AD(inv_d); g[2] = AD(0.0);
+    } else {
+        span = 3;
+        const double x0 = (double)lower * d, x1 = ((double)lower + 1.0) * d, x2 = ((double)lower + 2.0) * d;
+        AD s0 = xp - x0, s2 = xp - x2;
+        AD a0 = (s0.v < 0) ? -s0 : s0, a2 = (s2.v < 0) ? -s2 : s2;
+        AD t0 = (lp + d) - a0, t2 = (lp + d) - a2;
+        AD dl = lp * d;
+        w[0] = t0 * t0 / (dl * 4.0);
+        g[0] = (-t0 / (dl * 2.0) * s0) / a0;
+        AD s1 = xp - x1;
+        w[1] = 1.0 - (s1 * s1 + lp * lp) / (dl * 2.0);
+        g[1] = -s1 / dl;
+        w[2] = t2 * t2 / (dl * 4.0);
+        g[2] = (-t2 / (dl * 2.0) * s2) / a2;
+    }
+}
+
+// Isotropic tensor function f(b) = sum f_A(lambda) n_A n_A^T with dual lanes:
+// fA carries the lanes of the principal values (through the return map), the
+// off-diagonal lanes are D_AB (V^T db V)_AB with D_AB = (f_A - f_B)/(l_A - l_B)
+// or its coalescence limit lim_AB.
+GW_HD void spectral_assemble(const double V[3][3], const double lamb[3], const AD fA[3], const double lim[3][3],
+                             const double dbp[][3][3], AD out[3][3]) {
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+            double v = 0.0;
+            for (int A = 0; A < 3; ++A) v += fA[A].v * V[i][A] * V[j][A];
+            out[i][j] = AD(v);
+        }
+    double D[3][3];
+    for (int A = 0; A < 3; ++A)
+        for (int B = 0; B < 3; ++B) {
+            if (A == B) { D[A][B] = 0.0; continue; }
+            const double dl = lamb[A] - lamb[B];
+            const double sc = fmax(fabs(lamb[A]), fabs(lamb[B]));
+            D[A][B] = (fabs(dl) > 1e-9 * sc) ? (fA[A].v - fA[B].v) / dl : lim[A][B];
+        }
+    for (int l = 0; l < kAdjLanes; ++l) {
+        double M[3][3];
+        for (int A = 0; A < 3; ++A)
+            for (int B = 0; B < 3; ++B) M[A][B] = (A == B) ? fA[A].d[l] : D[A][B] * dbp[l][A][B];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int A = 0; A < 3; ++A)
+                    for (int B = 0; B < 3; ++B) v += V[i][A] * M[A][B] * V[j][B];
+                out[i][j].d[l] = v;
+            }
+    }
+}
+
+struct SolidDual {
+    AD r[9][2];        // residual rows per slot
+    AD F_new[3][3], b_new[3][3];
+    AD x_new[2], lp_new[2];
+    int nid[9];
+    double W[9], G[9][2];
+    int lower[2], span[2];
+    double xnew_dx[2];  // d lp_new_k / d x_new_k (clip branch: 0, +1 or -1)
+};
+
+// Forward pass of one 2D solid particle in dual arithmetic.  du: nodal
+// increments of the 9 slots (u_new - u_old), values only.
+GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lpv, const double *Fo_v,
+                             const double *bo_v, double Ev, const double fext[2], const double du[9][2], bool want_g2p,
+                             SolidDual &o) {
+    const gw_grid_t &g = c.g;
+    AD x[2] = {seed(xv[0], LX), seed(xv[1], LX + 1)};
+    AD lp[2] = {seed(lpv[0], LLP), seed(lpv[1], LLP + 1)};
+    AD Fo[3][3], bo[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) { Fo[i][j] = AD(Fo_v[i * 3 + j]); bo[i][j] = AD(bo_v[i * 3 + j]); }
+    Fo[0][0].d[LF] = 1.0; Fo[0][1].d[LF + 1] = 1.0; Fo[1][0].d[LF + 2] = 1.0; Fo[1][1].d[LF + 3] = 1.0;
+    Fo[2][2].d[LF + 4] = 1.0;
+    bo[0][0].d[LB] = 1.0; bo[0][1].d[LB + 1] = 1.0; bo[1][0].d[LB + 1] = 1.0; bo[1][1].d[LB + 2] = 1.0;
+    bo[2][2].d[LB + 3] = 1.0;
+    AD E = seed(Ev, LE);
+    const double nu = c.nu;
+    AD lam = E * (nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+    AD mu = E * (1.0 / (2.0 * (1.0 + nu)));
+
+    AD w[2][3], gw[2][3];
+    for (int k = 0; k < 2; ++k) gimp_axis_dual(x[k], lp[k], g.h[k], g.inv_h[k], o.lower[k], o.span[k], w[k], gw[k]);
+    AD W[9], G[9][2];
+    for (int a = 0; a < 9; ++a) {
+        const int i = a % 3, j = a / 3;
+        W[a] = w[0][i] * w[1][j];
+        G[a][0] = gw[0][i] * w[1][j];
+        G[a][1] = w[0][i] * gw[1][j];
+        o.W[a] = W[a].v;
+        o.G[a][0] = G[a][0].v;
+        o.G[a][1] = G[a][1].v;
+        const int cx = o.lower[0] + i, cy = o.lower[1] + j;
+        o.nid[a] = (cx >= 0 && cx <= g.n_grid[0] && cy >= 0 && cy <= g.n_grid[1]) ? cx + cy * (g.n_grid[0] + 1) : -1;
+    }
+    AD H[2][2], ubar(0.0);
+    for (int k = 0; k < 2; ++k)
+        for (int l = 0; l < 2; ++l) H[k][l] = AD(0.0);
+    AD dx_p[2] = {AD(0.0), AD(0.0)};
+    for (int a = 0; a < 9; ++a) {
+        if (o.nid[a] < 0) continue;
+        for (int k = 0; k < 2; ++k)
+            for (int l = 0; l < 2; ++l) H[k][l] += G[a][k] * du[a][l];
+        ubar += W[a] * du[a][1];
+        dx_p[0] += W[a] * du[a][0];
+        dx_p[1] += W[a] * du[a][1];
+    }
+    H[0][0].d[LH] += 1.0; H[0][1].d[LH + 1] += 1.0; H[1][0].d[LH + 2] += 1.0; H[1][1].d[LH + 3] += 1.0;
+    ubar.d[LU] += 1.0;
+
+    // kinematics
+    AD Finc[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Finc[i][j] = AD(i == j ? 1.0 : 0.0);
+    for (int i = 0; i < 2; ++i)
+        for (int j = 0; j < 2; ++j) Finc[i][j] += H[i][j];
+    AD det2 = Finc[0][0] * Finc[1][1] - Finc[0][1] * Finc[1][0];
+    AD Finv[2][2] = {{Finc[1][1] / det2, -Finc[0][1] / det2}, {-Finc[1][0] / det2, Finc[0][0] / det2}};
+    matmul3(Finc, Fo, o.F_new);
+    AD J = det3(o.F_new);
+    AD btr[3][3];
+    congruence3(Finc, bo, btr);
+
+    // stress (Kirchhoff) and b_new
+    AD tau[3][3];
+    const int model = c.mc.model;
+    if (model == GW_MODEL_HENCKY || model == GW_MODEL_J2 || model == GW_MODEL_DP) {
+        double B[3][3], lamb[3], V[3][3];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) B[i][j] = btr[i][j].v;
+        eig_sym3(B, lamb, V);
+        double dbp[kAdjLanes][3][3];
+        for (int l = 0; l < kAdjLanes; ++l) {
+            double T1[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j)
+                    T1[i][j] = btr[i][0].d[l] * V[0][j] + btr[i][1].d[l] * V[1][j] + btr[i][2].d[l] * V[2][j];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) dbp[l][i][j] = V[0][i] * T1[0][j] + V[1][i] * T1[1][j] + V[2][i] * T1[2][j];
+        }
+        AD etr[3], e[3], tA[3];
+        double etr_v[3];
+        for (int A = 0; A < 3; ++A) {
+            const bool ok = lamb[A] > 1e-8;
+            etr_v[A] = 0.5 * ::log(ok ? lamb[A] : 1e-8);
+            etr[A] = AD(etr_v[A]);
+            for (int l = 0; l < kAdjLanes; ++l) etr[A].d[l] = ok ? dbp[l][A][A] / (2.0 * lamb[A]) : 0.0;
+        }
+        if (model == GW_MODEL_J2) rm_j2<AD, double, AD>(etr, lam, mu, c.mc.kappa, e);
+        else if (model == GW_MODEL_DP) rm_dp<AD, double, AD>(etr, lam, mu, c.mc, e);
+        else for (int A = 0; A < 3; ++A) e[A] = etr[A];
+        tau_hencky(e, lam, mu, tA);
+        // coalescence limits from the value-level algorithmic tangent
+        double tv[3], dtau[3][4], ev[3], de[3][4], pn = 0.0;
+        principal_model<double>(c.mc, lam.v, mu.v, etr_v, 0.0, 0.0, pn, tv, dtau, ev, true, de);
+        double limT[3][3], limB[3][3];
+        AD fB[3];
+        for (int A = 0; A < 3; ++A) {
+            fB[A] = gexp(e[A] * 2.0);
+            for (int Bq = 0; Bq < 3; ++Bq) {
+                limT[A][Bq] = (dtau[A][A] - dtau[A][Bq]) / (2.0 * lamb[A]);
+                limB[A][Bq] = 2.0 * fB[A].v * (de[A][A] - de[A][Bq]) / (2.0 * lamb[A]);
+            }
+        }
+        spectral_assemble(V, lamb, tA, limT, dbp, tau);
+        spectral_assemble(V, lamb, fB, limB, dbp, o.b_new);
+    } else {
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) o.b_new[i][j] = btr[i][j];
+        if (model == GW_MODEL_NEOHOOKEAN) {  // J sigma = mu (F F^T - I) + lam ln J I
+            AD lnJ = glog(J);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    AD ff = o.F_new[i][0] * o.F_new[j][0] + o.F_new[i][1] * o.F_new[j][1] + o.F_new[i][2] * o.F_new[j][2];
+                    tau[i][j] = mu * (ff - (i == j ? 1.0 : 0.0));
+                    if (i == j) tau[i][j] += lam * lnJ;
+                }
+        } else {  // linear: sigma = lam tr(eps) I + 2 mu eps, tau = J sigma
+            AD eps[3][3];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) eps[i][j] = (o.F_new[i][j] + o.F_new[j][i]) * 0.5 - (i == j ? 1.0 : 0.0);
+            AD tr = eps[0][0] + eps[1][1] + eps[2][2];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    AD sg = mu * 2.0 * eps[i][j];
+                    if (i == j) sg += lam * tr;
+                    tau[i][j] = J * sg;
+                }
+        }
+    }
+
+    // residual rows (mpm/mpm_utils.py:575-596): r_a = -(Finv G_a)^T tau2 V0 + W_a rho0 V0 g + W_a f_ext + pen W_a
+    const double V0 = c.st.p_vol;
+    const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
+    const double gv = -c.st.gravity_mag * ramp;
+    AD pen(0.0);
+    bool pen_on = false;
+    if (c.st.has_footing) {
+        const double height = c.st.footing_initial_height + (c.st.current_step + 1.0) * c.st.footing_incr_disp;
+        if (xv[1] >= height && xv[0] > c.st.footing_min[0] && xv[0] < c.st.footing_max[0]) {
+            const double area = c.g.h[0] / c.st.PPD;
+            AD kp = E * (c.st.penalty_factor * area);
+            pen = -((height - (x[1] + ubar)) * kp);
+            if (c.st.footing_stable) pen = -pen;
+            pen_on = true;
+        }
+    }
+    for (int a = 0; a < 9; ++a) {
+        AD wg[2];
+        for (int i = 0; i < 2; ++i) wg[i] = Finv[i][0] * G[a][0] + Finv[i][1] * G[a][1];
+        for (int j = 0; j < 2; ++j) {
+            AD v = -(wg[0] * tau[0][j] + wg[1] * tau[1][j]) * V0;
+            if (j == 1) v += W[a] * (c.st.p_rho * V0 * gv);
+            if (j == 1 && pen_on) v += pen * W[a];
+            v += W[a] * fext[j];
+            o.r[a][j] = v;
+        }
+    }
+    if (!want_g2p) return;
+    // G2P outputs: x_new = x + sum W du ; lp_new from F_new columns, clipped
+    for (int k = 0; k < 2; ++k) o.x_new[k] = x[k] + dx_p[k];
+    for (int k = 0; k < 2; ++k) {
+        AD U = gsqrt(o.F_new[0][k] * o.F_new[0][k] + o.F_new[1][k] * o.F_new[1][k] + o.F_new[2][k] * o.F_new[2][k]);
+        AD v = U * c.st.lp0;
+        double dxd = 0.0;
+        if (o.x_new[k].v - v.v < c.g.domain_min[k]) { v = o.x_new[k] - (c.g.domain_min[k] + 1e-6); dxd = 1.0; }
+        if (o.x_new[k].v + v.v > c.g.domain_max[k]) { v = (c.g.domain_max[k] - 1e-6) - o.x_new[k]; dxd = -1.0; }
+        o.lp_new[k] = v;
+        o.xnew_dx[k] = dxd;
+    }
+}
+
+// ---------------------------------------------------------------- kernels
+struct AdjState {  // per-particle adjoint arrays (user order)
+    double *x, *lp, *F, *b, *E;  // [N*2], [N*2], [N*9], [N*9], [N]
+};
+
+// Adjoint G2P: seeds (x_new, lp_new, F_new, b_new) bars -> q_bar (written) and
+// the nodal adjoint u_bar (free DOFs of active rows, atomically accumulated).
+__global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__ u_new,
+                              const double *__restrict__ u_old, const uint8_t *__restrict__ free_mask, PtrsA A,
+                              AdjState seed_in, AdjState q_out, double *__restrict__ ubar_rows) {
+    const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= p.n) return;
+    double du[9][2];
+    {
+        int lower[2];
+        for (int k = 0; k < 2; ++k) lower[k] = cell_of(p.x[pid * 2 + k] - p.lp[pid * 2 + k], c.g.inv_h[k]);
+        for (int a = 0; a < 9; ++a) {
+            const int cx = lower[0] + a % 3, cy = lower[1] + a / 3;
+            const bool in = cx >= 0 && cx <= c.g.n_grid[0] && cy >= 0 && cy <= c.g.n_grid[1];
+            const int id = cx + cy * (c.g.n_grid[0] + 1);
+            for (int l = 0; l < 2; ++l) du[a][l] = in ? u_new[(size_t)id * 2 + l] - u_old[(size_t)id * 2 + l] : 0.0;
+        }
+    }
+    SolidDual o;
+    const double E = p.E ? p.E[pid] : c.E0;
+    const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
+    const bool ext = p.ext_flag && p.ext_flag[pid];
+    const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
+    solid2d_dual(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
+                 true, o);
+    AD s(0.0);
+    double xb_eff[2];
+    for (int k = 0; k < 2; ++k) {
+        const double xb = seed_in.x[pid * 2 + k], lb = seed_in.lp[pid * 2 + k];
+        s += o.x_new[k] * xb + o.lp_new[k] * lb;
+        xb_eff[k] = xb + lb * o.xnew_dx[k];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j)
+            s += o.F_new[i][j] * seed_in.F[(size_t)pid * 9 + i * 3 + j] + o.b_new[i][j] * seed_in.b[(size_t)pid * 9 + i * 3 + j];
+    // particle-input adjoints
+    q_out.x[pid * 2] = s.d[LX];
+    q_out.x[pid * 2 + 1] = s.d[LX + 1];
+    q_out.lp[pid * 2] = s.d[LLP];
+    q_out.lp[pid * 2 + 1] = s.d[LLP + 1];
+    double *Fq = q_out.F + (size_t)pid * 9, *bq = q_out.b + (size_t)pid * 9;
+    for (int k = 0; k < 9; ++k) { Fq[k] = 0.0; bq[k] = 0.0; }
+    Fq[0] = s.d[LF]; Fq[1] = s.d[LF + 1]; Fq[3] = s.d[LF + 2]; Fq[4] = s.d[LF + 3]; Fq[8] = s.d[LF + 4];
+    bq[0] = s.d[LB]; bq[1] = 0.5 * s.d[LB + 1]; bq[3] = 0.5 * s.d[LB + 1]; bq[4] = s.d[LB + 2]; bq[8] = s.d[LB + 3];
+    q_out.E[pid] = s.d[LE];
+    // nodal adjoint: H_bar_kl G_b,k on component l, plus W_b x_bar_eff
+    const double Hb[2][2] = {{s.d[LH], s.d[LH + 1]}, {s.d[LH + 2], s.d[LH + 3]}};
+    for (int b = 0; b < 9; ++b) {
+        const int id = o.nid[b];
+        if (id < 0) continue;
+        const uint8_t fm = free_mask[id];
+        if (!fm) continue;
+        const int row = A.node2row[id];
+        for (int l = 0; l < 2; ++l) {
+            if (!((fm >> l) & 1)) continue;
+            const double v = Hb[0][l] * o.G[b][0] + Hb[1][l] * o.G[b][1] + o.W[b] * xb_eff[l];
+            atomicAdd(&ubar_rows[(size_t)row * 2 + l], v);
+        }
+    }
+}
+
+// Adjoint P2G: q_bar += sum_a lambda_a . d r_a / d q over free DOFs.
+__global__ void k_adjoint_residual(LaunchConst c, PtrsP p, const double *__restrict__ u_new,
+                                   const double *__restrict__ u_old, const uint8_t *__restrict__ free_mask, PtrsA A,
+                                   const double *__restrict__ lambda_rows, AdjState q_out) {
+    const int pid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pid >= p.n) return;
+    double du[9][2];
+    {
+        int lower[2];
+        for (int k = 0; k < 2; ++k) lower[k] = cell_of(p.x[pid * 2 + k] - p.lp[pid * 2 + k], c.g.inv_h[k]);
+        for (int a = 0; a < 9; ++a) {
+            const int cx = lower[0] + a % 3, cy = lower[1] + a / 3;
+            const bool in = cx >= 0 && cx <= c.g.n_grid[0] && cy >= 0 && cy <= c.g.n_grid[1];
+            const int id = cx + cy * (c.g.n_grid[0] + 1);
+            for (int l = 0; l < 2; ++l) du[a][l] = in ? u_new[(size_t)id * 2 + l] - u_old[(size_t)id * 2 + l] : 0.0;
+        }
+    }
+    SolidDual o;
+    const double E = p.E ? p.E[pid] : c.E0;
+    const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
+    const bool ext = p.ext_flag && p.ext_flag[pid];
+    const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
+    solid2d_dual(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
+                 false, o);
+    AD s(0.0);
+    for (int a = 0; a < 9; ++a) {
+        const int id = o.nid[a];
+        if (id < 0) continue;
+        const uint8_t fm = free_mask[id];
+        if (!fm) continue;
+        const int row = A.node2row[id];
+        for (int f = 0; f < 2; ++f)
+            if ((fm >> f) & 1) s += o.r[a][f] * lambda_rows[(size_t)row * 2 + f];
+    }
+    q_out.x[pid * 2] += s.d[LX];
+    q_out.x[pid * 2 + 1] += s.d[LX + 1];
+    q_out.lp[pid * 2] += s.d[LLP];
+    q_out.lp[pid * 2 + 1] += s.d[LLP + 1];
+    double *Fq = q_out.F + (size_t)pid * 9, *bq = q_out.b + (size_t)pid * 9;
+    Fq[0] += s.d[LF]; Fq[1] += s.d[LF + 1]; Fq[3] += s.d[LF + 2]; Fq[4] += s.d[LF + 3]; Fq[8] += s.d[LF + 4];
+    bq[0] += s.d[LB]; bq[1] += 0.5 * s.d[LB + 1]; bq[3] += 0.5 * s.d[LB + 1]; bq[4] += s.d[LB + 2]; bq[8] += s.d[LB + 3];
+    q_out.E[pid] += s.d[LE];
+}
+
+// A^T with the same (symmetric) block pattern: block (r, c) of A^T is the
+// transpose of block (c, r) of A.
+template <int D, typename VT>
+__global__ void k_bsr_transpose(gw_grid_t g, PtrsA A, VT *__restrict__ AT) {
+    const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (r >= A.n_rows) return;
+    const int lane = threadIdx.x & 31;
+    const int nf = A.nf, node = A.row2node[r];
+    int ic[3] = {0, 0, 0};
+    {
+        int q = node;
+        for (int k = 0; k < D; ++k) { ic[k] = q % (g.n_grid[k] + 1); q /= (g.n_grid[k] + 1); }
+    }
+    const VT *vals = (const VT *)A.vals;
+    for (int j = A.row_ptr[r] + lane; j < A.row_ptr[r + 1]; j += 32) {
+        const int cr = A.cols[j];
+        const int cnode = A.row2node[cr];
+        int off[3] = {0, 0, 0}, q = cnode;
+        for (int k = 0; k < D; ++k) { off[k] = ic[k] - q % (g.n_grid[k] + 1); q /= (g.n_grid[k] + 1); }
+        const int slot = stencil_slot(A.stencil, A.mw, cnode, offset_bit<D>(off));
+        if (slot < 0) continue;
+        const VT *src = vals + (size_t)j * nf * nf;
+        VT *dst = AT + ((size_t)A.row_ptr[cr] + slot) * nf * nf;
+        for (int f = 0; f < nf; ++f)
+            for (int gg = 0; gg < nf; ++gg) dst[gg * nf + f] = src[f * nf + gg];
+    }
+}
+
+}  // namespace gw

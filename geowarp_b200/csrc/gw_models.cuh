@@ -40,23 +40,23 @@ inline MatConst make_matconst(const gw_material_t &m) {
     return c;
 }
 
-template <typename T, typename R>
-GW_HD void tau_hencky(const T e[3], R lam, R mu, T tau[3]) {
+template <typename T, typename LT>
+GW_HD void tau_hencky(const T e[3], LT lam, LT mu, T tau[3]) {
     T tr = e[0] + e[1] + e[2];
 #pragma unroll
-    for (int i = 0; i < 3; ++i) tau[i] = lam * tr + R(2) * mu * e[i];
+    for (int i = 0; i < 3; ++i) tau[i] = lam * tr + 2.0 * mu * e[i];
 }
 
 // ------------------------------------------------------------------ J2
-template <typename T, typename R>
-GW_HD void rm_j2(const T etr[3], R lam, R mu, R kappa, T e[3]) {
+template <typename T, typename R, typename LT>
+GW_HD void rm_j2(const T etr[3], LT lam, LT mu, R kappa, T e[3]) {
     T tau[3];
     tau_hencky(etr, lam, mu, tau);
     T P = (tau[0] + tau[1] + tau[2]) / R(3);
     T S[3] = {tau[0] - P, tau[1] - P, tau[2] - P};
     T nrm = gsqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]);
     if (val(nrm) > kappa) {
-        T dl = (nrm - kappa) / (R(2) * mu);
+        T dl = (nrm - kappa) / (2.0 * mu);
 #pragma unroll
         for (int i = 0; i < 3; ++i) e[i] = etr[i] - dl * (S[i] / nrm);
     } else {
@@ -108,8 +108,8 @@ GW_HD void dp_hess(const T S[3], const T &Q, R A, R sf, T H[3][3]) {
         }
 }
 
-template <typename T, typename R>
-GW_HD void dp_invariants(const T e[3], R lam, R mu, T tau[3], T &P, T S[3], T &Q) {
+template <typename T, typename R, typename LT>
+GW_HD void dp_invariants(const T e[3], LT lam, LT mu, T tau[3], T &P, T S[3], T &Q) {
     tau_hencky(e, lam, mu, tau);
     P = (tau[0] + tau[1] + tau[2]) / R(3);
 #pragma unroll
@@ -117,18 +117,29 @@ GW_HD void dp_invariants(const T e[3], R lam, R mu, T tau[3], T &P, T S[3], T &Q
     Q = gsqrt(S[0] * S[0] + S[1] * S[1] + S[2] * S[2]) * R(1.224744871391589);
 }
 
-template <typename T, typename R>
-GW_HD void rm_dp(const T etr[3], R lam, R mu, const MatConst &c, T e[3]) {
+template <typename T, typename R, typename LT>
+GW_HD void rm_dp(const T etr[3], LT lam, LT mu, const MatConst &c, T e[3]) {
     const R Af = R(c.A_phi), Bf = R(c.B_phi), Ap = R(c.A_psi), Bp = R(c.B_psi), sf = R(c.sf);
     T tau[3], P, S[3], Q;
-    dp_invariants(etr, lam, mu, tau, P, S, Q);
+    dp_invariants<T, R, LT>(etr, lam, mu, tau, P, S, Q);
 #pragma unroll
     for (int i = 0; i < 3; ++i) e[i] = etr[i];
     T y0 = dp_yield(P, Q, Af, Bf, sf);
     if (val(y0) < R(1e-10)) return;     // elastic
     if (c.dp_cutoff && val(P) >= R(0)) return;  // apex return not implemented in the reference (:347-349)
+    if (!c.dp_cutoff && Bf > R(0)) {
+        // extension: at or beyond the tip P_tip = A (1 - sf) / B no cone state is
+        // reachable; return to the tip (isotropic state), continuous with the cone return
+        const R p_tip = Af * (R(1) - sf) / Bf;
+        if (val(P) >= p_tip) {
+            const LT K3 = (lam + 2.0 * mu / 3.0) * 3.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) e[i] = T(R(0)) + p_tip / K3;
+            return;
+        }
+    }
     T dl = T(R(0));
-    const R a_d = lam + R(2) * mu, a_o = lam;  // elastic_a = lam 1 1^T + 2 mu I
+    const LT a_d = lam + 2.0 * mu, a_o = lam;  // elastic_a = lam 1 1^T + 2 mu I
     for (int it = 0; it < 10; ++it) {
         T gg[3], gf[3], hg[3][3];
         dp_grad(tau, Q, Ap, Bp, sf, gg);
@@ -156,7 +167,7 @@ GW_HD void rm_dp(const T etr[3], R lam, R mu, const MatConst &c, T e[3]) {
 #pragma unroll
         for (int i = 0; i < 3; ++i) e[i] = e[i] - x[i];
         dl = dl - x[3];
-        dp_invariants(e, lam, mu, tau, P, S, Q);
+        dp_invariants<T, R, LT>(e, lam, mu, tau, P, S, Q);
     }
 }
 
@@ -276,7 +287,7 @@ GW_HD void tau_norsand(const T e[3], const MatConst &c, T tau[3]) {
 // Outputs tau[A], dtau[A][lane], e_out[A]; pi_new updated for plastic NorSand.
 template <typename R>
 GW_HD void principal_model(const MatConst &c, R lam, R mu, const R etr_v[3], R eps_v_total, R pi_old, R &pi_new,
-                           R tau_v[3], R dtau[3][4], R e_out[3], bool want_tangent) {
+                           R tau_v[3], R dtau[3][4], R e_out[3], bool want_tangent, R (*de)[4] = nullptr) {
     typedef Dual<4, R> T;
     T etr[3], e[3], tau[3];
 #pragma unroll
@@ -288,11 +299,11 @@ GW_HD void principal_model(const MatConst &c, R lam, R mu, const R etr_v[3], R e
     if (want_tangent) evt.d[3] = R(1);
     switch (c.model) {
         case GW_MODEL_J2:
-            rm_j2(etr, lam, mu, R(c.kappa), e);
+            rm_j2<T, R, R>(etr, lam, mu, R(c.kappa), e);
             tau_hencky(e, lam, mu, tau);
             break;
         case GW_MODEL_DP:
-            rm_dp(etr, lam, mu, c, e);
+            rm_dp<T, R, R>(etr, lam, mu, c, e);
             tau_hencky(e, lam, mu, tau);
             break;
         case GW_MODEL_NORSAND: {
@@ -313,6 +324,9 @@ GW_HD void principal_model(const MatConst &c, R lam, R mu, const R etr_v[3], R e
         e_out[i] = e[i].v;
 #pragma unroll
         for (int l = 0; l < 4; ++l) dtau[i][l] = tau[i].d[l];
+        if (de)
+#pragma unroll
+            for (int l = 0; l < 4; ++l) de[i][l] = e[i].d[l];
     }
 }
 

@@ -289,6 +289,10 @@ GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const doub
             ev.kpen = E * c.st.penalty_factor * area;
             const double penetration = height - (xp[v] + s.ubar);
             ev.pen = -penetration * ev.kpen;
+            if (c.st.footing_stable) {  // attractive spring (extension)
+                ev.pen = -ev.pen;
+                ev.kpen = -ev.kpen;
+            }
             ev.pen_on = true;
         }
     }

@@ -330,6 +330,7 @@ class Engine:
             st.footing_initial_height = fo["initial_height"]
             st.footing_incr_disp = fo["incr_disp"]
             st.penalty_factor = fo["penalty_factor"]
+            st.footing_stable = 1 if fo.get("stable", False) else 0
         return st
 
     def assemble(self, mat_struct, current_step, total_steps, want_K=True):

@@ -25,9 +25,11 @@ def return_mapping(material_dict, e_trial, eps_v_total=None, pi_old=None, pi_new
 
     Returns (e_real [n,3], tau [n,3], dtau_de [n,3,3] or None, pi_new [n] or None).
     """
-    e_trial = e_trial.contiguous().to(torch.float64)
+    e_trial = e_trial.to(torch.float64).contiguous()
     n = e_trial.shape[0]
     dev = e_trial.device
+    f64 = lambda t: None if t is None else torch.as_tensor(t, device=dev).to(torch.float64).reshape(-1).contiguous()
+    eps_v_total, pi_old, pi_new = f64(eps_v_total), f64(pi_old), f64(pi_new)
     m = material_struct(material_dict)
     e_out = torch.empty_like(e_trial)
     tau = torch.empty_like(e_trial)

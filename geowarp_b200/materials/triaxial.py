@@ -34,10 +34,10 @@ def _run(md, trial, total, target, n_steps, rate, device, ns_state=None, tol=1e-
         for _it in range(n_iter):
             kw = {}
             if ns_state is not None:
-                kw = dict(eps_v_total=torch.tensor([total.sum()], device=device),
-                          pi_old=torch.tensor([ns_state[0]], device=device),
-                          pi_new=torch.tensor([ns_state[1]], device=device))
-            e, tau, dt, pn = return_mapping(md, torch.tensor(trial[None, :], device=device), tangent=True, **kw)
+                kw = dict(eps_v_total=torch.tensor([total.sum()], dtype=torch.float64, device=device),
+                          pi_old=torch.tensor([ns_state[0]], dtype=torch.float64, device=device),
+                          pi_new=torch.tensor([ns_state[1]], dtype=torch.float64, device=device))
+            e, tau, dt, pn = return_mapping(md, torch.tensor(trial[None, :], dtype=torch.float64, device=device), tangent=True, **kw)
             s = tau[0].cpu().numpy()
             rhs = np.array([target[0] - s[0], target[1] - s[1]])
             J = -dt[0].cpu().numpy()[:2, :2]
@@ -48,10 +48,10 @@ def _run(md, trial, total, target, n_steps, rate, device, ns_state=None, tol=1e-
                 break
         kw = {}
         if ns_state is not None:
-            kw = dict(eps_v_total=torch.tensor([total.sum()], device=device),
-                      pi_old=torch.tensor([ns_state[0]], device=device),
-                      pi_new=torch.tensor([ns_state[1]], device=device))
-        e, tau, _, pn = return_mapping(md, torch.tensor(trial[None, :], device=device), **kw)
+            kw = dict(eps_v_total=torch.tensor([total.sum()], dtype=torch.float64, device=device),
+                      pi_old=torch.tensor([ns_state[0]], dtype=torch.float64, device=device),
+                      pi_new=torch.tensor([ns_state[1]], dtype=torch.float64, device=device))
+        e, tau, _, pn = return_mapping(md, torch.tensor(trial[None, :], dtype=torch.float64, device=device), **kw)
         s = tau[0].cpu().numpy()
         if ns_state is not None:
             ns_state = (float(pn[0]), float(pn[0]))

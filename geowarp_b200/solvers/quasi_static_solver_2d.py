@@ -155,7 +155,8 @@ class quasi_static_solver_2d:
         if "penalty_factor" in ld:
             sp["footing"] = dict(min=(ld["footing_region_min_x"], 0.0), max=(ld["footing_region_max_x"], 0.0),
                                  initial_height=ld["footing_initial_height"], incr_disp=ld["footing_incr_disp"],
-                                 penalty_factor=ld["penalty_factor"])
+                                 penalty_factor=ld["penalty_factor"],
+                                 stable=bool(ld.get("footing_penalty_stable", False)))
         self.engine.step_params = sp
 
     @property

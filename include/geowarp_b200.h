@@ -106,7 +106,9 @@ typedef struct gw_step {
     double dt, phi_initial, mobility;   /* u-p only                               */
     double lp0;             /* GIMP_lp_initial                                    */
     int32_t has_footing;    /* penalty footing (mpm/mpm_utils.py:1234-1248)       */
-    int32_t pad0;
+    int32_t footing_stable; /* 0: the reference's residual k (z_new - h), a repulsive
+                               spring (negative stiffness); 1: k (h - z_new),
+                               attractive (extension, for the 2D strip footing) */
     double footing_min[2], footing_max[2];
     double footing_initial_height, footing_incr_disp, penalty_factor;
 } gw_step_t;
@@ -266,6 +268,42 @@ int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_particles_t *pt,
 int gw_return_map(const gw_material_t *mat, int32_t n, const double *e_trial, const double *eps_v_total,
                   const double *pi_old, double *pi_new, double *e_out, double *tau_out, double *dtau_de_out,
                   void *stream);
+
+/* ------------------------------------------------------------ adjoint (2D solid kind)
+ * The reference's only derivative is the Warp-tape gradient of the last
+ * residual w.r.t. a scalar Young's modulus at fixed state
+ * (solvers/quasi_static_coupled_solver_3d.py:159-165, 323-325).  These entry
+ * points give the total derivative of a load step instead: with u* solving
+ * R(u; q) = 0 for the particle inputs q = (x, lp, F_old, b_old, E),
+ *   q_bar = (d out/d q)^T out_bar + R_q^T lambda,  K^T lambda = (d out/d u)^T out_bar,
+ * out = (x_new, lp_new, F_new, b_new) the G2P outputs.  Per-particle arrays:
+ * x, lp [N*2]; F, b [N*9]; E [N]. */
+typedef struct gw_adjoint {
+    double *x, *lp, *F, *b, *E;
+} gw_adjoint_t;
+
+/* AT_vals: the values of A^T on A's (symmetric) block pattern. */
+int gw_bsr_transpose(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, void *AT_vals, void *stream);
+/* Adjoint G2P (mpm/mpm_utils.py:1351-1419, mpm/gimp.py:428-462): writes q_out
+ * (overwrites) and ubar_rows[n_rows*2] (free DOFs only). pt holds the state at
+ * the start of the load step, u_new the converged nodal solution. */
+int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st, const gw_particles_t *pt,
+                   const double *u_new, const double *u_old, const uint8_t *free_mask, const gw_bsr_t *A,
+                   const gw_adjoint_t *seed_in, gw_adjoint_t *q_out, double *ubar_rows, void *stream);
+/* Adjoint P2G of the residual (mpm/mpm_utils.py:416-780): q_out += R_q^T lambda. */
+int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st, const gw_particles_t *pt,
+                        const double *u_new, const double *u_old, const uint8_t *free_mask, const gw_bsr_t *A,
+                        const double *lambda_rows, gw_adjoint_t *q_out, void *stream);
+
+/* ------------------------------------------------------------ kernel timing
+ * Optional CUDA-event timing of the engine's main kernels (off by default):
+ * classes 0..7 = k_assemble, k_gm_spmv, k_gm_dots, k_gm_update, k_gm_next,
+ * k_g2p, k_adjoint_g2p, k_adjoint_residual.  gw_profile_read synchronises and
+ * returns the total time, launch count and algorithmic bytes of a class. */
+int gw_profile_enable(int32_t on);
+int gw_profile_reset(void);
+int gw_profile_read(int32_t cls, double *ms_total_host, int64_t *launches_host, double *bytes_host);
+const char *gw_profile_name(int32_t cls);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,67 @@
+"""Bounded CPU sample of the strip-footing workload for the benchmark's
+CPU-baseline leg (test infrastructure: the oracle is the checker, timed here
+only as the reported CPU baseline).
+
+One Newton iteration of load step 0 of the plane-strain Drucker-Prager strip
+footing: residual and complex-step element tangents for every particle
+(NumPy, single thread), global assembly and a SciPy sparse direct solve --
+the reference's 'scipy' solver path (solvers/quasi_static_solver_2d.py:214-220).
+"""
+import time
+
+import numpy as np
+from scipy.sparse.linalg import spsolve
+
+from .mpm import OracleEngine, init_particles_rectangle_2d
+
+
+def footing_oracle(n_cells_x=256, n_cells_y=128, dx=0.05, PPD=2, footing_width=1.0, pad=2):
+    n_grid_x, n_grid_y = n_cells_x + 2 * pad, n_cells_y + 2 * pad
+    sx, sy = pad * dx, pad * dx
+    ex, ey = sx + n_cells_x * dx, sy + n_cells_y * dx
+    x = init_particles_rectangle_2d(sx, sy, ex, ey, dx, n_grid_x, n_grid_y, PPD, n_cells_x * n_cells_y * PPD * PPD)
+    mat = dict(youngs_modulus=2e7, poisson_ratio=0.3, material_name="Drucker-Prager", friction_angle=30.0,
+               dilation_angle=0.0, cohesion=1e4, shape_factor=0.0, tension_cutoff=False)
+    xc = 0.5 * (sx + ex)
+    load = dict(gravity_mag=0.0, footing_region_min_x=xc - footing_width / 2, footing_region_max_x=xc + footing_width / 2,
+                footing_initial_height=ey - dx / (2 * PPD), footing_incr_disp=-0.2 / 100, penalty_factor=1000.0,
+                footing_penalty_stable=True)
+    grid = dict(n_grid=(n_grid_x, n_grid_y), h=(dx, dx), h_nodes=(dx, dx), domain_min=(sx, sy), domain_max=(ex, ey))
+    o = OracleEngine("solid2d", grid, x, (dx / PPD) ** 2, 2000.0, PPD, mat, load, lp0=dx / PPD / 2.0 - 1e-6,
+                     n_iter=20, tol=1e-6)
+    nn = (n_grid_x + 1) * (n_grid_y + 1)
+    ix = np.tile(np.arange(n_grid_x + 1), n_grid_y + 1)
+    iy = np.repeat(np.arange(n_grid_y + 1), n_grid_x + 1)
+    dof = ix + iy * (n_grid_x + 1)
+    side = (ix <= pad) | (ix >= pad + n_cells_x)
+    base = iy <= pad
+    o.boundary[dof[side | base]] = True
+    o.boundary[dof[base] + nn] = True
+    return o
+
+
+def oracle_newton_sample(footing_kwargs=None, full=(256, 128)):
+    """Seconds per Newton iteration of the full-size footing, estimated from a
+    timed Newton iteration of the 64x32-cell variant (or of the variant given in
+    footing_kwargs): the particle-local residual/tangent work scales with the
+    particle count, the sparse direct solve with DOFs^1.5 (2D nested dissection)."""
+    kw = dict(n_cells_x=64, n_cells_y=32, footing_width=0.25)
+    kw.update(footing_kwargs or {})
+    o = footing_oracle(**kw)
+    o.p2g()
+    t0 = time.perf_counter()
+    R, K, _ = o.assemble(0, 100)
+    t1 = time.perf_counter()
+    delta = spsolve(K.tocsc(), R)
+    t2 = time.perf_counter()
+    o.u_new += delta
+    n_full = full[0] * full[1] * 4
+    dof_full = 2 * (full[0] + 5) * (full[1] + 5)
+    pr = n_full / o.N
+    dr = dof_full / o.ndof
+    est = (t1 - t0) * pr + (t2 - t1) * dr ** 1.5
+    desc = (f"one Newton iteration (residual + complex-step element tangents {t1 - t0:.2f} s, SciPy spsolve "
+            f"{t2 - t1:.3f} s) of load step 0 of the {kw['n_cells_x']}x{kw['n_cells_y']}-cell variant "
+            f"({o.N} particles, {o.ndof} DOFs), NumPy oracle on 1 host thread; scaled to the 256x128-cell "
+            f"workload by x{pr:.0f} (particles) and x{dr ** 1.5:.0f} (solve)")
+    return est, desc

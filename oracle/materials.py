@@ -88,8 +88,11 @@ def return_map_dp(e_tr, lam, mu, phi, psi, c, sf, n_local=10, tension_cutoff=Tru
     Follows return_mapping_DruckerPrager, triaxial_DruckerPrager.py:308-412:
     elastic if f < 1e-10, trial state kept when P_trial >= 0 (apex return not
     implemented in the reference), else a 4x4 Newton in (e_1, e_2, e_3, dlambda).
-    tension_cutoff=False drops the P_trial >= 0 guard (extension: the cone
-    return then also acts in tension, which keeps the map continuous).
+    tension_cutoff=False replaces the P_trial >= 0 guard by a continuous
+    completion (extension): the cone return for P_trial below the tip of the
+    yield surface, P_tip = A (1 - sf) / B, and a return to the tip (isotropic
+    state at P_tip) at or beyond it, where the cone return with this flow rule
+    has no solution.
     """
     n = e_tr.shape[0]
     lam_v = np.broadcast_to(np.asarray(lam, dtype=np.float64).reshape(-1, 1), (n, 1))
@@ -106,6 +109,9 @@ def return_map_dp(e_tr, lam, mu, phi, psi, c, sf, n_local=10, tension_cutoff=Tru
     tau, P, S, Q = inv(e_tr)
     y0 = dp_yield(P, Q, phi, c, sf)
     elastic = (np.real(y0) < 1e-10) | ((np.real(P) >= 0.0) & tension_cutoff)
+    A_f, B_f = _dp_AB(phi, c)
+    p_tip = A_f * (1.0 - sf) / B_f if B_f > 0 else np.inf
+    apex = (~elastic) & (not tension_cutoff) & (np.real(P) >= p_tip)
     e = e_tr.copy()
     dl = np.zeros(e_tr.shape[0], dtype=e_tr.dtype)
     eye3 = np.eye(3)
@@ -125,6 +131,9 @@ def return_map_dp(e_tr, lam, mu, phi, psi, c, sf, n_local=10, tension_cutoff=Tru
         e = e - xd[:, :3]
         dl = dl - xd[:, 3]
         tau, P, S, Q = inv(e)
+    K = lam_v + 2.0 * mu_v / 3.0
+    e_apex = np.broadcast_to(p_tip / (3.0 * K), e_tr.shape)
+    e = np.where(apex[:, None], e_apex, e)
     return np.where(elastic[:, None], e_tr, e)
 
 

@@ -410,6 +410,8 @@ class OracleEngine:
             sel &= (xp[:, 1] > ld["footing_region_min_y"]) & (xp[:, 1] < ld["footing_region_max_y"])
         du = (W * dU[:, :, v]).sum(1)
         pen_res = -(height - (xp[:, v] + du)) * kpen
+        if ld.get("footing_penalty_stable", False):
+            pen_res = -pen_res  # attractive spring to the footing height (extension)
         pen_res = np.where(sel, pen_res, 0.0)
         return pen_res[:, None] * W, np.real(-pen_res[sel]).sum()
 

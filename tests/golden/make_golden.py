@@ -36,8 +36,8 @@ def bar(material, steps=5, n_steps=10):
                 iters=np.array(o.iters), steps=np.array([steps, n_steps]))
 
 
-def footing(steps=3, n_steps=10):
-    grid, parts, it, mat, load = cases.footing_dicts(nx=12, ny=6, n_steps=n_steps)
+def footing(steps=3, n_steps=10, **kw):
+    grid, parts, it, mat, load = cases.footing_dicts(nx=12, ny=6, n_steps=n_steps, **kw)
     o = cases.oracle_solid2d(grid, parts, it, mat, load)
     cases.footing_boundary(o.boundary, grid)
     forces = []
@@ -90,6 +90,7 @@ if __name__ == "__main__":
     save("bar_j2", **bar("J2"))
     save("bar_neohookean", **bar("Neo-Hookean"))
     save("footing_dp", **footing())
+    save("footing_dp_stable", **footing(stable=True, n_steps=100))
     save("terzaghi", **terzaghi())
     save("indentation3d", **indentation())
     save("jacobian_bar_j2", **jacobian_bar_j2())
