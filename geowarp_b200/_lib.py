@@ -39,7 +39,7 @@ class Material(C.Structure):
                 ("ns_kappa", C.c_double), ("ns_tilde_lambda", C.c_double), ("ns_M", C.c_double),
                 ("ns_N", C.c_double), ("ns_beta", C.c_double), ("ns_vc0", C.c_double), ("ns_p0", C.c_double),
                 ("ns_v0", C.c_double), ("ns_h", C.c_double), ("ns_shear_modulus", C.c_double),
-                ("ns_eps_v0", C.c_double)]
+                ("ns_eps_v0", C.c_double), ("dp_tip_tangent", C.c_double)]
 
 
 class Step(C.Structure):
@@ -50,7 +50,7 @@ class Step(C.Structure):
                 ("has_footing", C.c_int32), ("footing_stable", C.c_int32),
                 ("footing_min", C.c_double * 2), ("footing_max", C.c_double * 2),
                 ("footing_initial_height", C.c_double), ("footing_incr_disp", C.c_double),
-                ("penalty_factor", C.c_double)]
+                ("penalty_factor", C.c_double), ("gravity_full", C.c_int32), ("pad1", C.c_int32)]
 
 
 class Particles(C.Structure):
@@ -105,6 +105,7 @@ SIGNATURES = {
     "gw_g2p": (C.c_int, [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Particles), P, P, P]),
     "gw_return_map": (C.c_int, [C.POINTER(Material), I32, P, P, P, P, P, P, P, P]),
     "gw_profile_enable": (C.c_int, [I32]),
+    "gw_launch_count": (I64, []),
     "gw_profile_reset": (C.c_int, []),
     "gw_profile_read": (C.c_int, [I32, PD, C.POINTER(C.c_int64), PD]),
     "gw_profile_name": (C.c_char_p, [I32]),

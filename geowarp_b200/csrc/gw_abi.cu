@@ -70,6 +70,13 @@ struct ProfScope {
         if (r) cudaEventRecord(r->b, s);
     }
 };
+// every kernel launch of the library passes its grid size through here, so the
+// host can report how many launches a piece of work took (gw_launch_count)
+int64_t g_launches = 0;
+inline int gw_count_launch(int grid) {
+    ++g_launches;
+    return grid;
+}
 inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
 inline int red_grid_rows(int n_rows) { int b = nblk(n_rows, kThreads / 32); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
 inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
@@ -105,12 +112,12 @@ int scan_exclusive(const int *in, int *out, int n, int *ws, cudaStream_t s) {
     const int nb = (n + 1023) / 1024;
     int *sums = ws;
     int *sums_scan = ws + nb;
-    k_scan_block<<<nb, 1024, 0, s>>>(in, out, n, nb > 1 ? sums : nullptr);
+    k_scan_block<<<gw_count_launch(nb), 1024, 0, s>>>(in, out, n, nb > 1 ? sums : nullptr);
     GW_LAUNCHED();
     if (nb > 1) {
         int rc = scan_exclusive(sums, sums_scan, nb, ws + 2 * nb + 64, s);
         if (rc) return rc;
-        k_scan_add<<<nb, 1024, 0, s>>>(out, n, sums_scan);
+        k_scan_add<<<gw_count_launch(nb), 1024, 0, s>>>(out, n, sums_scan);
         GW_LAUNCHED();
     }
     return GW_OK;
@@ -175,8 +182,8 @@ extern "C" int gw_cell_sort(const gw_grid_t *grid, const gw_particles_t *pt, int
     int *valt = (int *)w; w += align256(4 * (int64_t)n);
     int *hist = (int *)w; w += align256(4 * 256 * (int64_t)nb);
     int *sws = (int *)w;
-    if (grid->dim == 2) k_cell_keys<2><<<nblk(n, kThreads), kThreads, 0, s>>>(*grid, pt->x, pt->lp, n, keys_out, perm_out);
-    else k_cell_keys<3><<<nblk(n, kThreads), kThreads, 0, s>>>(*grid, pt->x, pt->lp, n, keys_out, perm_out);
+    if (grid->dim == 2) k_cell_keys<2><<<gw_count_launch(nblk(n, kThreads)), kThreads, 0, s>>>(*grid, pt->x, pt->lp, n, keys_out, perm_out);
+    else k_cell_keys<3><<<gw_count_launch(nblk(n, kThreads)), kThreads, 0, s>>>(*grid, pt->x, pt->lp, n, keys_out, perm_out);
     GW_LAUNCHED();
     const int ncell = n_cells_of(*grid);
     int bits = 1;
@@ -185,11 +192,11 @@ extern "C" int gw_cell_sort(const gw_grid_t *grid, const gw_particles_t *pt, int
     int *kin = keys_out, *vin = perm_out, *kout = kalt, *vout = valt;
     for (int ps = 0; ps < passes; ++ps) {
         const int shift = 8 * ps;
-        k_radix_hist<<<nb, kThreads, 0, s>>>(kin, n, shift, nb, hist);
+        k_radix_hist<<<gw_count_launch(nb), kThreads, 0, s>>>(kin, n, shift, nb, hist);
         GW_LAUNCHED();
         int rc = scan_exclusive(hist, hist, 256 * nb, sws, s);
         if (rc) return rc;
-        k_radix_scatter<<<nb, kThreads, 0, s>>>(kin, vin, n, shift, nb, hist, kout, vout);
+        k_radix_scatter<<<gw_count_launch(nb), kThreads, 0, s>>>(kin, vin, n, shift, nb, hist, kout, vout);
         GW_LAUNCHED();
         int *t = kin; kin = kout; kout = t;
         t = vin; vin = vout; vout = t;
@@ -211,9 +218,9 @@ extern "C" int gw_p2g_activate(const gw_grid_t *grid, const gw_particles_t *pt, 
     uint32_t *cs = cell_span_u8;
     const int b = nblk(pt->n, kThreads);
     switch (grid->kind) {
-        case GW_KIND_SOLID2D: k_activate<GW_KIND_SOLID2D><<<b, kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
-        case GW_KIND_COUPLED2D: k_activate<GW_KIND_COUPLED2D><<<b, kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
-        case GW_KIND_COUPLED3D: k_activate<GW_KIND_COUPLED3D><<<b, kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
+        case GW_KIND_SOLID2D: k_activate<GW_KIND_SOLID2D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
+        case GW_KIND_COUPLED2D: k_activate<GW_KIND_COUPLED2D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
+        case GW_KIND_COUPLED3D: k_activate<GW_KIND_COUPLED3D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, perm, node_active, cs, boundary); break;
         default: return GW_EINVAL;
     }
     GW_LAUNCHED();
@@ -223,8 +230,8 @@ extern "C" int gw_p2g_activate(const gw_grid_t *grid, const gw_particles_t *pt, 
 extern "C" int gw_touched_nodes(const gw_grid_t *grid, const uint32_t *cell_span, uint8_t *touched, void *stream) {
     GW_REQUIRE(grid && cell_span && touched);
     const int nc = n_cells_of(*grid);
-    if (grid->dim == 2) k_touched<2><<<nblk(nc, kThreads), kThreads, 0, S(stream)>>>(*grid, cell_span, nc, touched);
-    else k_touched<3><<<nblk(nc, kThreads), kThreads, 0, S(stream)>>>(*grid, cell_span, nc, touched);
+    if (grid->dim == 2) k_touched<2><<<gw_count_launch(nblk(nc, kThreads)), kThreads, 0, S(stream)>>>(*grid, cell_span, nc, touched);
+    else k_touched<3><<<gw_count_launch(nblk(nc, kThreads)), kThreads, 0, S(stream)>>>(*grid, cell_span, nc, touched);
     GW_LAUNCHED();
     return GW_OK;
 }
@@ -240,16 +247,16 @@ extern "C" int gw_compact_rows(const gw_grid_t *grid, const uint8_t *node_active
     char *w = (char *)workspace;
     int *tmp = (int *)w; w += align256(4 * ((int64_t)n + 1));
     int *sws = (int *)w;
-    k_flags_to_int<<<nblk(n, kThreads), kThreads, 0, s>>>(node_active, n, tmp);
+    k_flags_to_int<<<gw_count_launch(nblk(n, kThreads)), kThreads, 0, s>>>(node_active, n, tmp);
     GW_LAUNCHED();
     int *last = sws;  // [0]: flag of the last node, [1]: number of active nodes
     GW_CUDA(cudaMemcpyAsync(last, tmp + (n - 1), 4, cudaMemcpyDeviceToDevice, s));
     int rc = scan_exclusive(tmp, tmp, n, sws + 64, s);
     if (rc) return rc;
-    k_compact<<<nblk(n, kThreads), kThreads, 0, s>>>(node_active, tmp, n, grid->nf, boundary, node2row, row2node,
+    k_compact<<<gw_count_launch(nblk(n, kThreads)), kThreads, 0, s>>>(node_active, tmp, n, grid->nf, boundary, node2row, row2node,
                                                      free_mask);
     GW_LAUNCHED();
-    k_add2<<<1, 32, 0, s>>>(tmp + (n - 1), last, last + 1);
+    k_add2<<<gw_count_launch(1), 32, 0, s>>>(tmp + (n - 1), last, last + 1);
     GW_LAUNCHED();
     int tot = 0;
     GW_CUDA(cudaMemcpyAsync(&tot, last + 1, 4, cudaMemcpyDeviceToHost, s));
@@ -268,9 +275,9 @@ extern "C" int gw_pattern_count(const gw_grid_t *grid, const uint32_t *cell_span
     GW_CUDA(cudaMemsetAsync(row_ptr, 0, 4 * ((size_t)n_rows + 1), s));
     if (n_rows > 0) {
         if (grid->dim == 2)
-            k_pattern_count<2><<<nblk(n_rows, kThreads), kThreads, 0, s>>>(*grid, cs, node2row, row2node, n_rows, mw, stencil, row_ptr);
+            k_pattern_count<2><<<gw_count_launch(nblk(n_rows, kThreads)), kThreads, 0, s>>>(*grid, cs, node2row, row2node, n_rows, mw, stencil, row_ptr);
         else
-            k_pattern_count<3><<<nblk(n_rows, kThreads), kThreads, 0, s>>>(*grid, cs, node2row, row2node, n_rows, mw, stencil, row_ptr);
+            k_pattern_count<3><<<gw_count_launch(nblk(n_rows, kThreads)), kThreads, 0, s>>>(*grid, cs, node2row, row2node, n_rows, mw, stencil, row_ptr);
         GW_LAUNCHED();
     }
     int rc = scan_exclusive(row_ptr, row_ptr, n_rows + 1, (int *)workspace, s);
@@ -286,8 +293,8 @@ extern "C" int gw_pattern_fill(const gw_grid_t *grid, const gw_bsr_t *A, int32_t
     GW_REQUIRE(grid && A && cols);
     if (A->n_rows == 0) return GW_OK;
     PtrsA a = make_ptrs(*A);
-    if (grid->dim == 2) k_pattern_fill<2><<<nblk(A->n_rows, kThreads), kThreads, 0, S(stream)>>>(*grid, a, cols);
-    else k_pattern_fill<3><<<nblk(A->n_rows, kThreads), kThreads, 0, S(stream)>>>(*grid, a, cols);
+    if (grid->dim == 2) k_pattern_fill<2><<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, S(stream)>>>(*grid, a, cols);
+    else k_pattern_fill<3><<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, S(stream)>>>(*grid, a, cols);
     GW_LAUNCHED();
     return GW_OK;
 }
@@ -304,14 +311,14 @@ extern "C" int gw_mass_assemble(const gw_grid_t *grid, const gw_particles_t *pt,
     PtrsA m = make_ptrs(*M);
     const int b = nblk(pt->n, kThreads);
     if (pt->n > 0) {
-        if (grid->kind == GW_KIND_COUPLED2D) k_mass<GW_KIND_COUPLED2D><<<b, kThreads, 0, s>>>(c, p, perm, m, rhs);
-        else if (grid->kind == GW_KIND_COUPLED3D) k_mass<GW_KIND_COUPLED3D><<<b, kThreads, 0, s>>>(c, p, perm, m, rhs);
+        if (grid->kind == GW_KIND_COUPLED2D) k_mass<GW_KIND_COUPLED2D><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, m, rhs);
+        else if (grid->kind == GW_KIND_COUPLED3D) k_mass<GW_KIND_COUPLED3D><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, m, rhs);
         else return GW_EINVAL;
         GW_LAUNCHED();
     }
     if (M->n_rows > 0) {
-        if (grid->dim == 2) k_mass_fix<2><<<nblk(M->n_rows, kThreads), kThreads, 0, s>>>(m);
-        else k_mass_fix<3><<<nblk(M->n_rows, kThreads), kThreads, 0, s>>>(m);
+        if (grid->dim == 2) k_mass_fix<2><<<gw_count_launch(nblk(M->n_rows, kThreads)), kThreads, 0, s>>>(m);
+        else k_mass_fix<3><<<gw_count_launch(nblk(M->n_rows, kThreads)), kThreads, 0, s>>>(m);
         GW_LAUNCHED();
     }
     return GW_OK;
@@ -322,7 +329,7 @@ extern "C" int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_
                                      double *u_old, double *u_new, void *stream) {
     GW_REQUIRE(grid && mass_row2node && p_hat && boundary && u_old && u_new);
     if (n_mass_rows == 0) return GW_OK;
-    k_set_nodal_pressure<<<nblk(n_mass_rows, kThreads), kThreads, 0, S(stream)>>>(
+    k_set_nodal_pressure<<<gw_count_launch(nblk(n_mass_rows, kThreads)), kThreads, 0, S(stream)>>>(
         n_mass_rows, mass_row2node, p_hat, boundary, grid->kind == GW_KIND_COUPLED3D ? node_active : nullptr,
         grid->n_nodes, grid->nf, u_old, u_new);
     GW_LAUNCHED();
@@ -342,17 +349,18 @@ int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const
         // (F_new, b_new, sigma), nodal gather (2 x NS x NF doubles), residual and
         // the element blocks scattered into the matrix (span^D x span^D blocks)
         const double per_p = 8.0 * (2 * D + 9 + 9 + 1) + 8.0 * 27 + 8.0 * 2 * NS * NF + 8.0 * NS * NF;
-        const double mat = A ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
+        const bool want_K = A->vals != nullptr;
+        const double mat = want_K ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
         ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + mat);
-        if (!A) k_assemble<KIND, false, double><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-        else if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-        else k_assemble<KIND, true, float><<<b, kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        if (!want_K) k_assemble<KIND, false, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        else if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        else k_assemble<KIND, true, float><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         GW_LAUNCHED();
     }
-    if (A && A->n_rows > 0) {
+    if (A->vals && A->n_rows > 0) {
         const int D = KindTraits<KIND>::D;
-        if (prec == GW_PREC_F64) k_identity_dirichlet<D, double><<<nblk(A->n_rows, kThreads), kThreads, 0, s>>>(a, fm);
-        else k_identity_dirichlet<D, float><<<nblk(A->n_rows, kThreads), kThreads, 0, s>>>(a, fm);
+        if (prec == GW_PREC_F64) k_identity_dirichlet<D, double><<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, s>>>(a, fm);
+        else k_identity_dirichlet<D, float><<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, s>>>(a, fm);
         GW_LAUNCHED();
     }
     return GW_OK;
@@ -364,19 +372,19 @@ extern "C" int gw_assemble(const gw_grid_t *grid, const gw_material_t *mat, cons
                            const double *u_new, const double *u_old, const gw_bsr_t *A, int32_t prec, double *R_rows,
                            double *force, void *stream) {
     GW_REQUIRE(grid && mat && st && pt && perm && free_mask && u_new && u_old && R_rows);
+    // the row map is needed for the residual even without a matrix
+    GW_REQUIRE(A && A->node2row && (A->n_rows == 0 || A->row2node));
     GW_REQUIRE(mat->model >= 0 && mat->model <= GW_MODEL_NORSAND);
     cudaStream_t s = S(stream);
     LaunchConst c = make_lc(grid, mat, st);
     PtrsP p = make_ptrs(*pt);
-    gw_bsr_t dummy;
-    memset(&dummy, 0, sizeof(dummy));
-    // the row map and stencil are needed for the residual even without a matrix
-    PtrsA a = make_ptrs(A ? *A : dummy);
-    if (A) {
+    PtrsA a = make_ptrs(*A);
+    if (A->vals) {
+        GW_REQUIRE(A->row_ptr && A->cols && A->stencil);
         const size_t vb = (prec == GW_PREC_F64 ? 8 : 4) * (size_t)A->nnzb * A->nf * A->nf;
         GW_CUDA(cudaMemsetAsync(A->vals, 0, vb, s));
-        GW_CUDA(cudaMemsetAsync(R_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
     }
+    GW_CUDA(cudaMemsetAsync(R_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
     switch (grid->kind) {
         case GW_KIND_SOLID2D: return launch_assemble<GW_KIND_SOLID2D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
         case GW_KIND_COUPLED2D: return launch_assemble<GW_KIND_COUPLED2D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
@@ -426,11 +434,11 @@ int krylov(const gw_bsr_t *A, int method, int precond, const double *b, double *
     memset(&h, 0, sizeof(h));
     h.max_iter = max_iter;
     GW_CUDA(cudaMemcpyAsync(&k.sc->max_iter, &h.max_iter, sizeof(int), cudaMemcpyHostToDevice, s));
-    k_precond_setup<NF, VT><<<nblk(nr, kThreads), kThreads, 0, s>>>(a, D, precond, k.Minv);
+    k_precond_setup<NF, VT><<<gw_count_launch(nblk(nr, kThreads)), kThreads, 0, s>>>(a, D, precond, k.Minv);
     GW_LAUNCHED();
     const int gw_rows = red_grid_rows(nr), ge_rows = red_grid_elems(nr);
-    if (method == GW_KRYLOV_CG) k_cg_init<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V, rtol);
-    else k_bicg_init<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V, rtol);
+    if (method == GW_KRYLOV_CG) k_cg_init<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V, rtol);
+    else k_bicg_init<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V, rtol);
     GW_LAUNCHED();
     int chunk = 2;
     for (;;) {
@@ -439,15 +447,15 @@ int krylov(const gw_bsr_t *A, int method, int precond, const double *b, double *
         if (h.done) break;
         for (int it = 0; it < chunk; ++it) {
             if (method == GW_KRYLOV_CG) {
-                k_cg_p<NF><<<red_grid_elems((int64_t)nr * NF), kThreads, 0, s>>>(nr, V);
-                k_cg_q<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V);
-                k_cg_xr<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
+                k_cg_p<NF><<<gw_count_launch(red_grid_elems((int64_t)nr * NF)), kThreads, 0, s>>>(nr, V);
+                k_cg_q<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V);
+                k_cg_xr<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
             } else {
-                k_bicg_p<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
-                k_bicg_v<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V);
-                k_bicg_s<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
-                k_bicg_t<NF, VT><<<gw_rows, kThreads, 0, s>>>(a, V);
-                k_bicg_xr<NF><<<ge_rows, kThreads, 0, s>>>(nr, V);
+                k_bicg_p<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
+                k_bicg_v<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V);
+                k_bicg_s<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
+                k_bicg_t<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V);
+                k_bicg_xr<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
             }
         }
         GW_LAUNCHED();
@@ -502,15 +510,15 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
     struct { int max_iter, restart; } lim = {max_iter, restart};
     GW_CUDA(cudaMemcpyAsync(&G.sc->max_iter, &lim, sizeof(lim), cudaMemcpyHostToDevice, s));
     const int D = (A->mask_words == 1) ? 2 : 3;
-    k_precond_setup<NF, VT><<<nblk(nr, kThreads), kThreads, 0, s>>>(a, D, precond, G.Minv);
+    k_precond_setup<NF, VT><<<gw_count_launch(nblk(nr, kThreads)), kThreads, 0, s>>>(a, D, precond, G.Minv);
     GW_LAUNCHED();
     const int gr = red_grid_rows(nr), ge = red_grid_elems(nr), gv = red_grid_elems(n);
     GScalars h;
     memset(&h, 0, head);
     int first = 1;
     for (int cycle = 0; cycle < 1000000; ++cycle) {
-        k_gm_residual<NF, VT><<<gr, kThreads, 0, s>>>(a, G, first, rtol);
-        k_gm_next<NF><<<ge, kThreads, 0, s>>>(nr, G, 1);
+        k_gm_residual<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, first, rtol);
+        k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 1);
         GW_LAUNCHED();
         first = 0;
         GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
@@ -522,12 +530,12 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
         for (;;) {
             for (int it = 0; it < chunk; ++it, ++kk) {
                 const double vb = 8.0 * n * (kk + 2);
-                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv<NF, VT><<<gr, kThreads, 0, s>>>(a, G); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gv, kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gv, kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gv, kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gv, kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_NEXT, s, 8.0 * n * 3 + 8.0 * nr * NF * NF); k_gm_next<NF><<<ge, kThreads, 0, s>>>(nr, G, 0); }
+                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G); }
+                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
+                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
+                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_NEXT, s, 8.0 * n * 3 + 8.0 * nr * NF * NF); k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 0); }
             }
             GW_LAUNCHED();
             GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
@@ -536,8 +544,8 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
             chunk = chunk < 32 ? chunk * 2 : 32;
         }
         if (h.status) break;
-        k_gm_solve_y<<<1, 32, 0, s>>>(G.sc);
-        k_gm_update_x<NF><<<ge, kThreads, 0, s>>>(nr, G);
+        k_gm_solve_y<<<gw_count_launch(1), 32, 0, s>>>(G.sc);
+        k_gm_update_x<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G);
         GW_LAUNCHED();
     }
     *iters = h.iters;
@@ -608,8 +616,8 @@ int spmv_any(const gw_bsr_t *A, const double *x, double *y, bool trans, cudaStre
     if (trans) GW_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
 #define GW_SPMV_CASE(NF_)                                                  \
     case NF_:                                                              \
-        if (trans) k_spmv_t<NF_, VT><<<g, kThreads, 0, s>>>(a, x, y);      \
-        else k_spmv<NF_, VT><<<g, kThreads, 0, s>>>(a, x, y);              \
+        if (trans) k_spmv_t<NF_, VT><<<gw_count_launch(g), kThreads, 0, s>>>(a, x, y);      \
+        else k_spmv<NF_, VT><<<gw_count_launch(g), kThreads, 0, s>>>(a, x, y);              \
         break;
     switch (A->nf) {
         GW_SPMV_CASE(1) GW_SPMV_CASE(2) GW_SPMV_CASE(3) GW_SPMV_CASE(4)
@@ -636,7 +644,7 @@ extern "C" int gw_norm2(const double *v, int32_t n, double *norm_dev, void *work
     double *partials = (double *)workspace;
     unsigned *ticket = (unsigned *)((char *)workspace + align256(8 * kRedBlocks));
     GW_CUDA(cudaMemsetAsync(ticket, 0, sizeof(unsigned), S(stream)));
-    k_norm2<<<red_grid_elems(n), kThreads, 0, S(stream)>>>(v, n, partials, ticket, norm_dev);
+    k_norm2<<<gw_count_launch(red_grid_elems(n)), kThreads, 0, S(stream)>>>(v, n, partials, ticket, norm_dev);
     GW_LAUNCHED();
     return GW_OK;
 }
@@ -644,7 +652,7 @@ extern "C" int gw_norm2(const double *v, int32_t n, double *norm_dev, void *work
 extern "C" int gw_apply_increment(const gw_bsr_t *A, const double *delta, double *u_full, void *stream) {
     GW_REQUIRE(A && delta && u_full);
     if (A->n_rows == 0) return GW_OK;
-    k_apply_increment<<<nblk(A->n_rows, kThreads), kThreads, 0, S(stream)>>>(A->n_rows, A->nf, A->row2node, delta, u_full);
+    k_apply_increment<<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, S(stream)>>>(A->n_rows, A->nf, A->row2node, delta, u_full);
     GW_LAUNCHED();
     return GW_OK;
 }
@@ -660,9 +668,9 @@ extern "C" int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_parti
     ProfScope ps(PC_G2P, S(stream), (double)pt->n * 8.0 * (2 * grid->dim * 3 + 9 * 4 + 3) +
                                         (double)pt->n * 27.0 * 8.0 * grid->nf * 2);
     switch (grid->kind) {
-        case GW_KIND_SOLID2D: k_g2p<GW_KIND_SOLID2D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
-        case GW_KIND_COUPLED2D: k_g2p<GW_KIND_COUPLED2D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
-        case GW_KIND_COUPLED3D: k_g2p<GW_KIND_COUPLED3D><<<b, kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
+        case GW_KIND_SOLID2D: k_g2p<GW_KIND_SOLID2D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
+        case GW_KIND_COUPLED2D: k_g2p<GW_KIND_COUPLED2D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
+        case GW_KIND_COUPLED3D: k_g2p<GW_KIND_COUPLED3D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
         default: return GW_EINVAL;
     }
     GW_LAUNCHED();
@@ -678,7 +686,7 @@ extern "C" int gw_return_map(const gw_material_t *mat, int32_t n, const double *
     MatConst mc = make_matconst(*mat);
     const double nu = mat->poisson_ratio, E = mat->youngs_modulus;
     const double lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), mu = E / (2.0 * (1.0 + nu));
-    k_return_map<<<nblk(n, kThreads), kThreads, 0, S(stream)>>>(mc, lam, mu, n, e_trial, eps_v_total, pi_old, pi_new,
+    k_return_map<<<gw_count_launch(nblk(n, kThreads)), kThreads, 0, S(stream)>>>(mc, lam, mu, n, e_trial, eps_v_total, pi_old, pi_new,
                                                                 e_out, tau_out, dtau_de_out);
     GW_LAUNCHED();
     return GW_OK;
@@ -702,11 +710,11 @@ extern "C" int gw_bsr_transpose(const gw_grid_t *grid, const gw_bsr_t *A, int32_
     GW_CUDA(cudaMemsetAsync(AT_vals, 0, vb, s));
     const int b = nblk(A->n_rows, kThreads / 32);
     if (grid->dim == 2) {
-        if (prec == GW_PREC_F64) k_bsr_transpose<2, double><<<b, kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
-        else k_bsr_transpose<2, float><<<b, kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
+        if (prec == GW_PREC_F64) k_bsr_transpose<2, double><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
+        else k_bsr_transpose<2, float><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
     } else {
-        if (prec == GW_PREC_F64) k_bsr_transpose<3, double><<<b, kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
-        else k_bsr_transpose<3, float><<<b, kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
+        if (prec == GW_PREC_F64) k_bsr_transpose<3, double><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
+        else k_bsr_transpose<3, float><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
     }
     GW_LAUNCHED();
     return GW_OK;
@@ -723,8 +731,9 @@ extern "C" int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, c
     GW_CUDA(cudaMemsetAsync(ubar_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
     if (pt->n == 0) return GW_OK;
     LaunchConst c = make_lc(grid, mat, st);
+    c.mc.tip_tangent = 0.0;  // exact derivatives of the converged state
     ProfScope ps(PC_ADJ_G2P, s, (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 18 + 23 + 2 * 9 * 2));
-    k_adjoint_g2p<<<nblk(pt->n, 128), 128, 0, s>>>(c, make_ptrs(*pt), u_new, u_old, free_mask, make_ptrs(*A),
+    k_adjoint_g2p<<<gw_count_launch(nblk(pt->n, 128)), 128, 0, s>>>(c, make_ptrs(*pt), u_new, u_old, free_mask, make_ptrs(*A),
                                                  make_adj(*seed_in), make_adj(*q_out), ubar_rows);
     GW_LAUNCHED();
     return GW_OK;
@@ -739,14 +748,17 @@ extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *m
     if (mat->model == GW_MODEL_NORSAND) return GW_EMODEL;
     if (pt->n == 0) return GW_OK;
     LaunchConst c = make_lc(grid, mat, st);
+    c.mc.tip_tangent = 0.0;  // exact derivatives of the converged residual
     ProfScope ps(PC_ADJ_RES, S(stream), (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 23 * 2 + 2 * 9 * 2 + 9 * 2));
-    k_adjoint_residual<<<nblk(pt->n, 128), 128, 0, S(stream)>>>(c, make_ptrs(*pt), u_new, u_old, free_mask,
+    k_adjoint_residual<<<gw_count_launch(nblk(pt->n, 128)), 128, 0, S(stream)>>>(c, make_ptrs(*pt), u_new, u_old, free_mask,
                                                                 make_ptrs(*A), lambda_rows, make_adj(*q_out));
     GW_LAUNCHED();
     return GW_OK;
 }
 
 // ==================================================================== kernel timing
+extern "C" int64_t gw_launch_count(void) { return g_launches; }
+
 extern "C" int gw_profile_enable(int32_t on) {
     g_prof_on = on != 0;
     return GW_OK;

@@ -232,7 +232,7 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
     // residual rows (mpm/mpm_utils.py:575-596): r_a = -(Finv G_a)^T tau2 V0 + W_a rho0 V0 g + W_a f_ext + pen W_a
     const double V0 = c.st.p_vol;
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
-    const double gv = -c.st.gravity_mag * ramp;
+    const double gv = -c.st.gravity_mag * (c.st.gravity_full ? 1.0 : ramp);
     AD pen(0.0);
     bool pen_on = false;
     if (c.st.has_footing) {

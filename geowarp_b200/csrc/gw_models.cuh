@@ -19,6 +19,7 @@ struct MatConst {
     double kappa;                  // J2
     double A_phi, B_phi, A_psi, B_psi, sf;  // DP (triaxial_DruckerPrager.py:130-134, 151-155)
     double ns_kappa, ns_tl, ns_M, ns_N, ns_beta, ns_vc0, ns_p0, ns_v0, ns_h, ns_mu, ns_ev0;
+    double tip_tangent;            // DP: Jacobian-only elastic fraction at the cone tip
 };
 
 inline MatConst make_matconst(const gw_material_t &m) {
@@ -37,6 +38,7 @@ inline MatConst make_matconst(const gw_material_t &m) {
     c.ns_kappa = m.ns_kappa; c.ns_tl = m.ns_tilde_lambda; c.ns_M = m.ns_M; c.ns_N = m.ns_N;
     c.ns_beta = m.ns_beta; c.ns_vc0 = m.ns_vc0; c.ns_p0 = m.ns_p0; c.ns_v0 = m.ns_v0; c.ns_h = m.ns_h;
     c.ns_mu = m.ns_shear_modulus; c.ns_ev0 = m.ns_eps_v0;
+    c.tip_tangent = m.dp_tip_tangent;
     return c;
 }
 
@@ -133,8 +135,11 @@ GW_HD void rm_dp(const T etr[3], LT lam, LT mu, const MatConst &c, T e[3]) {
         const R p_tip = Af * (R(1) - sf) / Bf;
         if (val(P) >= p_tip) {
             const LT K3 = (lam + 2.0 * mu / 3.0) * 3.0;
+            // the tip state is fixed (zero exact tangent); a nonzero tip_tangent keeps
+            // that fraction of the trial strain's derivative, value unchanged
+            const R frac = R(c.tip_tangent);
 #pragma unroll
-            for (int i = 0; i < 3; ++i) e[i] = T(R(0)) + p_tip / K3;
+            for (int i = 0; i < 3; ++i) e[i] = T(R(0)) + p_tip / K3 + frac * (etr[i] - val(etr[i]));
             return;
         }
     }

@@ -454,7 +454,7 @@ GW_HD void residual_rows(const LaunchConst &c, const PState<KIND> &s, const PEva
     }
     const double Vn = V0 * ev.J;
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
-    const double gv = -c.st.gravity_mag * ramp;
+    const double gv = -c.st.gravity_mag * (c.st.gravity_full ? 1.0 : ramp);
     const double pb = UP ? s.pbar : 0.0;
     double rho;
     if (UP) {

@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(kThreads) k_assemble(LaunchConst c, PtrsP p, c
     for (int k = 0; k < D; ++k)
         if (s.sh.ax[k].lower < 0 || s.sh.ax[k].lower >= c.g.n_grid[k]) { atomicOr(&g_status, ST_RANGE); return; }
     VT *vals = (VT *)A.vals;
-    const double gv = -c.st.gravity_mag * ramp;
+    const double gv = -c.st.gravity_mag * (c.st.gravity_full ? 1.0 : ramp);
     for (int b = 0; b < NS; ++b) {
         const int idb = s.nid[b];
         if (idb < 0 || !s.sh.in_span(b)) continue;

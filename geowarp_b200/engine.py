@@ -54,6 +54,7 @@ def material_struct(mat):
     m.cohesion = float(mat.get("cohesion", 0.0))
     m.shape_factor = float(mat.get("shape_factor", 0.0))
     m.dp_tension_cutoff = 1 if mat.get("tension_cutoff", True) else 0
+    m.dp_tip_tangent = float(mat.get("tip_tangent_fraction", 0.0))
     m.ns_kappa = float(mat.get("kappa", 0.0)) if name == "NorSand" else 0.0
     for key, attr in (("tilde_lambda", "ns_tilde_lambda"), ("M", "ns_M"), ("N", "ns_N"), ("beta", "ns_beta"),
                       ("vc0", "ns_vc0"), ("p0", "ns_p0"), ("v0", "ns_v0"), ("h", "ns_h"),
@@ -179,6 +180,8 @@ class Engine:
         self.m_rows = 0
         self.m_nnzb = 0
         self.step_params = {}
+        self.line_search_growth = None  # e.g. 2.0 enables the backtracking safeguard
+        self.line_search_max = 6
         self.log = []  # per Newton iteration: (step, it, ||R||, krylov iters, relres, status)
 
     # ------------------------------------------------------------------ structs
@@ -312,6 +315,7 @@ class Engine:
         st.current_step = float(current_step)
         st.total_steps = float(total_steps)
         st.gravity_mag = float(sp.get("gravity_mag", 0.0))
+        st.gravity_full = 0 if sp.get("gravity_ramp", True) else 1
         for k in range(3):
             st.point_load[k] = float(sp.get("point_load", (0.0, 0.0, 0.0))[k])
             st.traction[k] = float(sp.get("traction", (0.0, 0.0, 0.0))[k])
@@ -337,12 +341,12 @@ class Engine:
         g, pt, s = self.grid_struct(), self.particles_struct(), self.stream
         st = self.step_struct(current_step, total_steps)
         A = self.bsr_struct()
-        n = self.n_rows * self.nf
+        if not want_K:
+            A.vals = None  # residual only: the row map is still required
         self.force.zero_()
-        self._R[:n].zero_()
         L.call("gw_assemble", C.byref(g), C.byref(mat_struct), C.byref(st), C.byref(pt), _p(self.perm),
-               _p(self.free_mask), _p(self.u_new), _p(self.u_old), C.byref(A) if want_K else None, self.prec,
-               _p(self._R), _p(self.force), s)
+               _p(self.free_mask), _p(self.u_new), _p(self.u_old), C.byref(A), self.prec, _p(self._R),
+               _p(self.force), s)
 
     def residual_norm_async(self):
         n = self.n_rows * self.nf
@@ -387,12 +391,35 @@ class Engine:
     def newton(self, mat_struct, current_step, total_steps, n_iter, tol):
         """Newton loop with the reference's stopping rule
         (solvers/quasi_static_solver_2d.py:151-231): R is assembled before the
-        update, the update is applied, then ||R|| < tol stops the loop."""
+        update, the update is applied, then ||R|| < tol stops the loop.
+
+        With line_search_growth set (extension, off by default), an iterate
+        whose residual norm exceeds growth x the previous one is rejected and
+        the previous Newton step is halved (at most line_search_max times per
+        load step); accepted iterates follow the reference exactly."""
         its = 0
+        growth = self.line_search_growth
+        prev = None  # (u before the last step, delta, ||R|| at u)
+        n_bt = 0
+        alpha = 1.0
+        n = self.n_rows * self.nf
         for it in range(n_iter):
             self.assemble(mat_struct, current_step, total_steps, want_K=True)
             self.residual_norm_async()
+            if growth:
+                nrm = float(self.norm_dev.item())
+                if prev is not None and (not math.isfinite(nrm) or nrm > growth * prev[2]) and n_bt < self.line_search_max:
+                    alpha *= 0.5
+                    n_bt += 1
+                    self.u_new.copy_(prev[0])
+                    self._delta[:n].copy_(prev[1]).mul_(alpha)
+                    self.apply_increment()
+                    self.log.append((current_step, it, nrm, 0, alpha, "backtrack"))
+                    continue
             kit, relres, rc = self.krylov()
+            if growth:
+                prev = (self.u_new.clone(), self._delta[:n].clone(), nrm)
+                alpha = 1.0
             self.apply_increment()
             nrm = float(self.norm_dev.item())
             its += 1

@@ -151,7 +151,7 @@ class quasi_static_solver_2d:
         ld = self.load_dict
         sp = dict(gravity_mag=self.gravity_mag, point_load=(self.point_load_value_x, self.point_load_value_y, 0.0),
                   traction=(0.0, 0.0, 0.0), p_vol=self.p_vol, p_rho=self.p_rho, PPD=self.PPD,
-                  lp0=self.GIMP_lp_initial)
+                  lp0=self.GIMP_lp_initial, gravity_ramp=bool(ld.get("gravity_ramp", True)))
         if "penalty_factor" in ld:
             sp["footing"] = dict(min=(ld["footing_region_min_x"], 0.0), max=(ld["footing_region_max_x"], 0.0),
                                  initial_height=ld["footing_initial_height"], incr_disp=ld["footing_incr_disp"],

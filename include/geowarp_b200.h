@@ -94,6 +94,10 @@ typedef struct gw_material {
     /* NorSand (triaxial_NorSand.py:13-43) */
     double ns_kappa, ns_tilde_lambda, ns_M, ns_N, ns_beta, ns_vc0, ns_p0, ns_v0, ns_h;
     double ns_shear_modulus, ns_eps_v0;
+    double dp_tip_tangent;  /* DP with dp_tension_cutoff 0 (extension): fraction of the
+                               elastic tangent that particles returned to the cone tip
+                               contribute to the Jacobian (their exact tangent is zero;
+                               0 = exact).  The residual is not changed. */
 } gw_material_t;
 
 typedef struct gw_step {
@@ -111,6 +115,10 @@ typedef struct gw_step {
                                attractive (extension, for the 2D strip footing) */
     double footing_min[2], footing_max[2];
     double footing_initial_height, footing_incr_disp, penalty_factor;
+    int32_t gravity_full;   /* 0: gravity ramped by (step+1)/total_steps as in the
+                               reference; 1: full gravity in every load step (extension,
+                               for soil that starts from a geostatic stress state) */
+    int32_t pad1;
 } gw_step_t;
 
 /* Particle state, user order.  x, lp: [N*dim]; F*, b*, sigma: [N*9] row-major
@@ -211,8 +219,10 @@ int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_row2node, i
  * assemble_residual_coupled_3d_neohookean (:1020-1294) and the coloured
  * reverse-AD Jacobian (solvers/quasi_static_solver_2d.py:169-198 and
  * solvers/sparse_differentiation.py).  One thread per particle (cell order)
- * evaluates the residual and, when A != NULL, its exact element tangent
+ * evaluates the residual and, when A->vals != NULL, its exact element tangent
  * K = -dR/du, scattered element-by-element into A->vals (precision = prec).
+ * A is always required: its row map (node2row) places the residual rows;
+ * A->vals == NULL asks for the residual only.
  * R_rows[n_rows*nf] (FP64) receives the masked residual; Dirichlet and
  * inactive DOFs get identity rows (mpm/mpm_utils.py:1299-1341).
  * force_host_accum: device double[1] accumulating the penalty footing force.
@@ -302,6 +312,9 @@ int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *mat, const g
  * returns the total time, launch count and algorithmic bytes of a class. */
 int gw_profile_enable(int32_t on);
 int gw_profile_reset(void);
+/* Number of kernels the library has launched since it was loaded (host
+ * counter; no counterpart in the reference, which launches through Warp). */
+int64_t gw_launch_count(void);
 int gw_profile_read(int32_t cls, double *ms_total_host, int64_t *launches_host, double *bytes_host);
 const char *gw_profile_name(int32_t cls);
 

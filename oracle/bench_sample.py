@@ -15,7 +15,25 @@ from scipy.sparse.linalg import spsolve
 from .mpm import OracleEngine, init_particles_rectangle_2d
 
 
-def footing_oracle(n_cells_x=256, n_cells_y=128, dx=0.05, PPD=2, footing_width=1.0, pad=2):
+def geostatic_b(y, surface_y, rho, gravity, E, nu, K0):
+    """Elastic left Cauchy-Green tensors of the geostatic state sigma_yy =
+    -rho g (surface_y - y), sigma_xx = sigma_zz = K0 sigma_yy (Hencky law
+    inverted with J = 1)."""
+    lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu))
+    mu = E / (2.0 * (1.0 + nu))
+    syy = -rho * gravity * (surface_y - np.asarray(y, dtype=np.float64))
+    tau = np.stack([K0 * syy, syy, K0 * syy], axis=-1)
+    eps = (tau - lam * tau.sum(-1, keepdims=True) / (3.0 * lam + 2.0 * mu)) / (2.0 * mu)
+    b = np.zeros(eps.shape[:-1] + (3, 3))
+    for i in range(3):
+        b[..., i, i] = np.exp(2.0 * eps[..., i])
+    return b
+
+
+def footing_oracle(n_cells_x=256, n_cells_y=128, dx=0.05, PPD=2, footing_width=1.0, pad=2, gravity=9.81):
+    """The strip-footing workload: Drucker-Prager soil (E 2e7 Pa, nu 0.3,
+    c 10 kPa, phi 30, psi 0) with self-weight at full magnitude from the first
+    load step, starting from the K0 = 1 - sin(phi) geostatic state."""
     n_grid_x, n_grid_y = n_cells_x + 2 * pad, n_cells_y + 2 * pad
     sx, sy = pad * dx, pad * dx
     ex, ey = sx + n_cells_x * dx, sy + n_cells_y * dx
@@ -23,9 +41,9 @@ def footing_oracle(n_cells_x=256, n_cells_y=128, dx=0.05, PPD=2, footing_width=1
     mat = dict(youngs_modulus=2e7, poisson_ratio=0.3, material_name="Drucker-Prager", friction_angle=30.0,
                dilation_angle=0.0, cohesion=1e4, shape_factor=0.0, tension_cutoff=False)
     xc = 0.5 * (sx + ex)
-    load = dict(gravity_mag=0.0, footing_region_min_x=xc - footing_width / 2, footing_region_max_x=xc + footing_width / 2,
-                footing_initial_height=ey - dx / (2 * PPD), footing_incr_disp=-0.2 / 100, penalty_factor=1000.0,
-                footing_penalty_stable=True)
+    load = dict(gravity_mag=gravity, gravity_ramp=False, footing_region_min_x=xc - footing_width / 2,
+                footing_region_max_x=xc + footing_width / 2, footing_initial_height=ey - dx / (2 * PPD),
+                footing_incr_disp=-0.2 / 100, penalty_factor=1000.0, footing_penalty_stable=True)
     grid = dict(n_grid=(n_grid_x, n_grid_y), h=(dx, dx), h_nodes=(dx, dx), domain_min=(sx, sy), domain_max=(ex, ey))
     o = OracleEngine("solid2d", grid, x, (dx / PPD) ** 2, 2000.0, PPD, mat, load, lp0=dx / PPD / 2.0 - 1e-6,
                      n_iter=20, tol=1e-6)
@@ -37,6 +55,8 @@ def footing_oracle(n_cells_x=256, n_cells_y=128, dx=0.05, PPD=2, footing_width=1
     base = iy <= pad
     o.boundary[dof[side | base]] = True
     o.boundary[dof[base] + nn] = True
+    if gravity > 0.0:
+        o.b_old = geostatic_b(o.x[:, 1], ey, 2000.0, gravity, 2e7, 0.3, 1.0 - np.sin(np.radians(30.0)))
     return o
 
 
@@ -65,3 +85,41 @@ def oracle_newton_sample(footing_kwargs=None, full=(256, 128)):
             f"({o.N} particles, {o.ndof} DOFs), NumPy oracle on 1 host thread; scaled to the 256x128-cell "
             f"workload by x{pr:.0f} (particles) and x{dr ** 1.5:.0f} (solve)")
     return est, desc
+
+
+def oracle_load_step_sample(footing_kwargs=None, full=(256, 128), step=0):
+    """Seconds per load step of the full-size footing, from one complete load
+    step (P2G, Newton to the tolerance, G2P) of the 64x32-cell variant:
+    residual/tangent assembly scaled by the particle count, each sparse direct
+    solve by DOFs^1.5.  Returns (seconds, Newton iterations, description)."""
+    import scipy.sparse.linalg as sla
+    from . import mpm as M
+    kw = dict(n_cells_x=64, n_cells_y=32, footing_width=0.25)
+    kw.update(footing_kwargs or {})
+    o = footing_oracle(**kw)
+    t_solve = [0.0]
+    orig = M.spsolve
+
+    def timed_spsolve(A, b):
+        t = time.perf_counter()
+        x = sla.spsolve(A, b)
+        t_solve[0] += time.perf_counter() - t
+        return x
+
+    M.spsolve = timed_spsolve
+    try:
+        t0 = time.perf_counter()
+        o.advance_one_step(step, 100)
+        total = time.perf_counter() - t0
+    finally:
+        M.spsolve = orig
+    its = o.iters[-1] if getattr(o, "iters", None) else 1
+    n_full = full[0] * full[1] * 4
+    dof_full = 2 * (full[0] + 5) * (full[1] + 5)
+    pr, dr = n_full / o.N, dof_full / o.ndof
+    est = (total - t_solve[0]) * pr + t_solve[0] * dr ** 1.5
+    desc = (f"one complete load step ({its} Newton iterations; residual + complex-step tangents "
+            f"{total - t_solve[0]:.2f} s, SciPy spsolve {t_solve[0]:.3f} s) of load step {step} of the "
+            f"{kw['n_cells_x']}x{kw['n_cells_y']}-cell variant ({o.N} particles, {o.ndof} DOFs), NumPy oracle on "
+            f"1 host thread; scaled to the 256x128-cell workload by x{pr:.0f} (particles) and x{dr ** 1.5:.0f} (solve)")
+    return est, its, desc

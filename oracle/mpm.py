@@ -341,7 +341,8 @@ class OracleEngine:
         sig = sig3[:, :D, :D]
         V_new = self.p_vol * J
         g = np.zeros(D)
-        g[D - 1] = -self.load.get("gravity_mag", 0.0) * ramp
+        # gravity_ramp False (extension): full gravity from the first load step
+        g[D - 1] = -self.load.get("gravity_mag", 0.0) * (ramp if self.load.get("gravity_ramp", True) else 1.0)
         Ggrad = np.einsum("nkl,nal->nak", Finv, Gr)  # incr_F_inv @ weight_GRAD
         r = np.zeros(Uloc_new.shape[:2] + (self.nf,), dtype=np.result_type(dtype, sig))
         fext = np.zeros((self.N, D))

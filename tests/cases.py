@@ -64,11 +64,15 @@ def oracle_solid2d(grid, parts, it, mat, load):
 
 # ---------------------------------------------------------------- 2D solid: DP strip footing (small)
 def footing_dicts(nx=16, ny=8, dx=0.05, E=2e7, nu=0.3, c=1e4, phi=30.0, psi=0.0, width=0.2, total_disp=0.02,
-                  n_steps=10, penalty=1000.0, rho=2000.0, g=0.0, n_iter=15, tol=1e-6, stable=False):
+                  n_steps=10, penalty=1000.0, rho=2000.0, g=0.0, n_iter=15, tol=1e-6, stable=False, geostatic=False):
     """Plane-strain rigid strip footing on Drucker-Prager soil: a soil block of
     nx x ny cells (2x2 particles per cell) in an (nx+4) x (ny+4) grid, rollers
     on the sides, fixed base, penalty footing of the given width centred on the
-    top surface, displacement-controlled over n_steps."""
+    top surface, displacement-controlled over n_steps.  geostatic: self-weight
+    g = 9.81 at full magnitude from the first step (the caller sets the K0
+    initial state)."""
+    if geostatic:
+        g = 9.81
     n_grid_x, n_grid_y = nx + 4, ny + 4
     start_x, start_y = 2 * dx, 2 * dx
     end_x, end_y = start_x + nx * dx, start_y + ny * dx
@@ -84,7 +88,8 @@ def footing_dicts(nx=16, ny=8, dx=0.05, E=2e7, nu=0.3, c=1e4, phi=30.0, psi=0.0,
     load = dict(gravity_mag=g, traction_value_x=0.0, traction_value_y=0.0, point_load_value_x=0.0,
                 point_load_value_y=0.0, footing_region_min_x=xc - width / 2, footing_region_max_x=xc + width / 2,
                 footing_initial_height=end_y - dx / (2 * PPD) if stable else end_y - dx / PPD,
-                footing_incr_disp=-total_disp / n_steps, penalty_factor=penalty, footing_penalty_stable=stable)
+                footing_incr_disp=-total_disp / n_steps, penalty_factor=penalty, footing_penalty_stable=stable,
+                gravity_ramp=not geostatic)
     return grid, parts, it, mat, load
 
 

@@ -18,6 +18,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.dirname(HERE))
 
 import cases  # noqa: E402
+from oracle.bench_sample import geostatic_b  # noqa: E402
 from oracle.triaxial import triaxial_dp, triaxial_norsand  # noqa: E402
 
 
@@ -40,6 +41,9 @@ def footing(steps=3, n_steps=10, **kw):
     grid, parts, it, mat, load = cases.footing_dicts(nx=12, ny=6, n_steps=n_steps, **kw)
     o = cases.oracle_solid2d(grid, parts, it, mat, load)
     cases.footing_boundary(o.boundary, grid)
+    if kw.get("geostatic"):
+        o.b_old = geostatic_b(o.x[:, 1], grid["end_y"], parts["p_rho"], load["gravity_mag"], mat["youngs_modulus"],
+                              mat["poisson_ratio"], 1.0 - np.sin(np.radians(mat["friction_angle"])))
     forces = []
     for k in range(steps):
         o.advance_one_step(k, n_steps)
@@ -91,6 +95,7 @@ if __name__ == "__main__":
     save("bar_neohookean", **bar("Neo-Hookean"))
     save("footing_dp", **footing())
     save("footing_dp_stable", **footing(stable=True, n_steps=100))
+    save("footing_dp_geostatic", **footing(stable=True, n_steps=100, geostatic=True))
     save("terzaghi", **terzaghi())
     save("indentation3d", **indentation())
     save("jacobian_bar_j2", **jacobian_bar_j2())

@@ -119,6 +119,30 @@ def test_footing_dp_stable_matches_golden(cuda):
     assert np.abs(np.array(forces) - g["force"]).max() <= 1e-9 * np.abs(g["force"]).max()
 
 
+def test_footing_dp_geostatic_matches_golden(cuda):
+    """The benchmark's soil state: self-weight at full magnitude from the first
+    load step (gravity_ramp=False) and the K0 geostatic start set by
+    problems.geostatic_stress, against the oracle's own restatement."""
+    import os
+    from geowarp_b200 import problems
+    from geowarp_b200.solvers import quasi_static_solver_2d
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "footing_dp_geostatic.npz"))
+    grid, parts, it, mat, load = cases.footing_dicts(nx=12, ny=6, n_steps=100, stable=True, geostatic=True)
+    s = quasi_static_solver_2d(grid, parts, it, mat, load)
+    b = np.zeros(s.n_matrix_size, dtype=bool)
+    cases.footing_boundary(b, grid)
+    s.dofStruct.boundary_flag_array[:] = torch.as_tensor(b, device=s.x_particles.device)
+    problems.geostatic_stress(s, grid["end_y"], parts["p_rho"], load["gravity_mag"],
+                              1.0 - np.sin(np.radians(mat["friction_angle"])))
+    forces = []
+    for k in range(3):
+        s.advance_one_step(k, 100)
+        forces.append(s.footing_force)
+    assert rel_err(s.x_particles.cpu().numpy() - g["x0"], g["x"] - g["x0"]) < 1e-9
+    assert rel_err(s.particle_Cauchy_stress_array.cpu().numpy(), g["sigma"]) < 1e-9
+    assert np.abs(np.array(forces) - g["force"]).max() <= 1e-9 * np.abs(g["force"]).max()
+
+
 def test_sort_is_stable_and_deterministic(cuda):
     s = run_gpu_bar("Hencky elasticity", 1, 10, height=6.25)
     e = s.engine

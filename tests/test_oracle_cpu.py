@@ -129,3 +129,35 @@ def test_triaxial_dp_reaches_the_cone():
     M = 6 * np.sin(phi) / (3 - np.sin(phi))
     assert abs(g["Q"][-1] / g["P"][-1] - M) < 2e-3 * M
     assert np.all(np.diff(g["Q"][:4]) > 0)
+
+
+def test_geostatic_state_inverts_hencky_and_is_in_equilibrium():
+    """The K0 geostatic start of the footing workload: the product's and the
+    oracle's left Cauchy-Green tensors agree, reproduce sigma_yy = -rho g depth
+    and K0 sigma_yy through the Hencky law, and give a small initial residual
+    compared with the self-weight (cpGIMP integrates the linear stress field
+    of the layer exactly, so the discrete state is in equilibrium)."""
+    import torch
+    from geowarp_b200.problems import geostatic_left_cauchy_green
+    from oracle.bench_sample import geostatic_b
+    E, nu, K0, rho, g = 2e7, 0.3, 0.5, 2000.0, 9.81
+    y = np.linspace(0.1, 1.2, 23)
+    b_o = geostatic_b(y, 1.3, rho, g, E, nu, K0)
+    b_p = geostatic_left_cauchy_green(torch.as_tensor(y), 1.3, rho, g, E, nu, K0).numpy()
+    assert np.abs(b_o - b_p).max() < 1e-15
+    lam, mu = E * nu / ((1 + nu) * (1 - 2 * nu)), E / (2 * (1 + nu))
+    eps = 0.5 * np.log(np.diagonal(b_o, axis1=1, axis2=2))
+    tau = lam * eps.sum(-1, keepdims=True) + 2 * mu * eps
+    syy = -rho * g * (1.3 - y)
+    assert np.abs(tau[:, 1] - syy).max() < 1e-9 * rho * g
+    assert np.abs(tau[:, 0] - K0 * syy).max() < 1e-9 * rho * g
+    # equilibrium of the small geostatic footing block before the footing moves
+    grid, parts, it, mat, load = cases.footing_dicts(nx=12, ny=6, n_steps=100, stable=True, geostatic=True)
+    load = dict(load, footing_incr_disp=0.0)
+    o = cases.oracle_solid2d(grid, parts, it, mat, load)
+    cases.footing_boundary(o.boundary, grid)
+    o.b_old = geostatic_b(o.x[:, 1], grid["end_y"], rho, g, E, nu, K0)
+    o.p2g()
+    R, _, _ = o.assemble(0, 100, want_K=False)
+    weight = rho * g * parts["p_vol"] * parts["n_particles"]
+    assert np.linalg.norm(R) < 1e-9 * weight
