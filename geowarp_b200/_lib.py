@@ -96,6 +96,8 @@ SIGNATURES = {
                               C.POINTER(Bsr), I32, P, P, P]),
     "gw_krylov_workspace_bytes": (I64, [I32, I32, I32]),
     "gw_bsr_krylov_solve": (C.c_int, [C.POINTER(Bsr), I32, I32, I32, P, P, C.c_double, I32, P, PI32, PD, P]),
+    "gw_krylov_static_max_unknowns": (I64, []),
+    "gw_bsr_krylov_solve_static": (C.c_int, [C.POINTER(Bsr), I32, I32, I32, P, P, C.c_double, I32, PI32, PD, P]),
     "gw_gmres_workspace_bytes": (I64, [I32, I32, I32]),
     "gw_bsr_gmres_solve": (C.c_int, [C.POINTER(Bsr), I32, I32, P, P, C.c_double, I32, I32, P, PI32, PD, P]),
     "gw_bsr_spmv": (C.c_int, [C.POINTER(Bsr), I32, P, P, P]),

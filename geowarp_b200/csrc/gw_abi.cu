@@ -607,6 +607,77 @@ extern "C" int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t meth
     return rc;
 }
 
+// ==================================================================== Krylov without a caller workspace
+// For callers that cannot allocate device memory themselves: a host whose own
+// memory manager owns the device heap, or a code path where calling cudaMalloc
+// is not allowed.  The scratch the BiCGSTAB / CG driver needs lives in one
+// file-scope device array, sized for at most kStaticKrylovMaxUnknowns unknowns
+// (n_rows * nf); every GPU that loads the library holds it (about 12.6 MB)
+// until the process exits.
+namespace {
+constexpr int64_t kStaticKrylovMaxUnknowns = 131072;
+constexpr int64_t align256c(int64_t b) { return (b + 255) & ~(int64_t)255; }
+// krylov_ws_bytes at the limit, for the largest block size (nf = 4)
+constexpr int64_t kStaticKrylovBytes = 8 * align256c(8 * kStaticKrylovMaxUnknowns) +
+                                       align256c(8 * kStaticKrylovMaxUnknowns * 4) +
+                                       align256c(8 * (int64_t)kRedBlocks * 4) + align256c(sizeof(KScalars));
+static __device__ __align__(256) unsigned char g_krylov_scratch[kStaticKrylovBytes];
+
+constexpr int kMaxStaticDevices = 64;
+void *g_krylov_scratch_addr[kMaxStaticDevices] = {};
+
+// Device address of g_krylov_scratch on the current device.  The name is only a
+// host-side stand-in, so the address is looked up once per device, with that
+// device current, and cached.
+int static_krylov_scratch(void **out) {
+    int dev = 0;
+    GW_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxStaticDevices) {
+        snprintf(g_msg, sizeof(g_msg), "gw_bsr_krylov_solve_static: device ordinal %d above %d", dev,
+                 kMaxStaticDevices - 1);
+        return GW_EINVAL;
+    }
+    void *p = __atomic_load_n(&g_krylov_scratch_addr[dev], __ATOMIC_ACQUIRE);
+    if (!p) {
+        GW_CUDA(cudaGetSymbolAddress(&p, g_krylov_scratch));
+        __atomic_store_n(&g_krylov_scratch_addr[dev], p, __ATOMIC_RELEASE);
+    }
+    *out = p;
+    return GW_OK;
+}
+}  // namespace
+
+extern "C" int64_t gw_krylov_static_max_unknowns(void) { return kStaticKrylovMaxUnknowns; }
+
+extern "C" int gw_bsr_krylov_solve_static(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond,
+                                          const double *b, double *x, double rtol, int32_t max_iter,
+                                          int32_t *iters_host, double *relres_host, void *stream) {
+    GW_REQUIRE(A && b && x && iters_host && relres_host && max_iter > 0);
+    const int64_t unknowns = (int64_t)A->n_rows * A->nf;
+    if (A->n_rows < 0 || A->nf < 1 || A->nf > 4 || unknowns > kStaticKrylovMaxUnknowns ||
+        krylov_ws_bytes(A->n_rows, A->nf) > kStaticKrylovBytes) {
+        snprintf(g_msg, sizeof(g_msg),
+                 "gw_bsr_krylov_solve_static: %lld unknowns (n_rows %d x nf %d) exceed the static scratch limit of "
+                 "%lld unknowns; use gw_bsr_krylov_solve with a caller workspace",
+                 (long long)unknowns, A->n_rows, A->nf, (long long)kStaticKrylovMaxUnknowns);
+        return GW_EINVAL;
+    }
+    void *ws = nullptr;
+    const int rs = static_krylov_scratch(&ws);
+    if (rs != GW_OK) return rs;
+    // the driver clears the scalar block (reduction ticket, flags) on every call
+    // and writes every vector before reading it, so the contents a previous call
+    // left in the scratch are never used
+    int it = 0;
+    double rr = 0.0;
+    int rc = (prec == GW_PREC_F64)
+                 ? krylov_nf<double>(A, method, precond, b, x, rtol, max_iter, ws, &it, &rr, S(stream))
+                 : krylov_nf<float>(A, method, precond, b, x, rtol, max_iter, ws, &it, &rr, S(stream));
+    *iters_host = it;
+    *relres_host = rr;
+    return rc;
+}
+
 namespace {
 template <typename VT>
 int spmv_any(const gw_bsr_t *A, const double *x, double *y, bool trans, cudaStream_t s) {

@@ -242,6 +242,24 @@ int64_t gw_krylov_workspace_bytes(int32_t n_rows, int32_t nf, int32_t prec);
 int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond, const double *b, double *x,
                         double rtol, int32_t max_iter, void *workspace, int32_t *iters_host, double *relres_host,
                         void *stream);
+/* gw_bsr_krylov_solve without a workspace argument (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc: a host whose own
+ * memory manager owns the device heap, or a path on which allocating device
+ * memory is not allowed.  The solver's scratch is a file-scope device array in
+ * the library, about 12.6 MB on every GPU that loads it, held until the
+ * process exits; the call allocates nothing.  Limit:
+ * n_rows * nf <= gw_krylov_static_max_unknowns() (131072); larger systems
+ * return GW_EINVAL with a message naming the limit.  The first call on a
+ * device looks up the array's device address with that device current (the
+ * stream must belong to the current device); make that first call before any
+ * stream capture.  All calls on a device share the one array: every call
+ * clears the part that must start at zero, but calls that overlap on the GPU
+ * (other streams, other host threads) race on it and must be serialised by
+ * the caller. */
+int64_t gw_krylov_static_max_unknowns(void);
+int gw_bsr_krylov_solve_static(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond, const double *b,
+                               double *x, double rtol, int32_t max_iter, int32_t *iters_host, double *relres_host,
+                               void *stream);
 /* Restarted right-preconditioned GMRES(restart), restart <= 128: the robust
  * solver for the nonsymmetric, indefinite Jacobians (penalty footing, u-p
  * saddle point) on which BiCGSTAB breaks down.  Classical Gram-Schmidt with
