@@ -345,13 +345,15 @@ int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const
     const int b = nblk(p.n, kThreads);
     if (p.n > 0) {
         const int D = KindTraits<KIND>::D, NF = KindTraits<KIND>::NF, NS = KindTraits<KIND>::NS;
-        // algorithmic bytes: particle state in (x, lp, F_old, b_old, E), state out
-        // (F_new, b_new, sigma), nodal gather (2 x NS x NF doubles), residual and
-        // the element blocks scattered into the matrix (span^D x span^D blocks)
-        const double per_p = 8.0 * (2 * D + 9 + 9 + 1) + 8.0 * 27 + 8.0 * 2 * NS * NF + 8.0 * NS * NF;
+        // algorithmic bytes, each array once: particle state in (x, lp, F_old,
+        // b_old, E) and out (F_new, b_new, sigma), the grid vectors (u_new, u_old,
+        // R) and the matrix values
+        (void)NS;
+        const double per_p = 8.0 * (2 * D + 9 + 9 + 1) + 8.0 * 27;
+        const double grid = 8.0 * 3 * (double)A->n_rows * NF;
         const bool want_K = A->vals != nullptr;
         const double mat = want_K ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
-        ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + mat);
+        ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + grid + mat);
         if (!want_K) k_assemble<KIND, false, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         else if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         else k_assemble<KIND, true, float><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
