@@ -67,6 +67,15 @@ class Bsr(C.Structure):
                 ("stencil", C.c_void_p), ("vals", C.c_void_p)]
 
 
+MG_MAX_LEVELS = 20
+
+
+class MgPlan(C.Structure):
+    _fields_ = [("levels", C.c_int32), ("dense_n", C.c_int32), ("n_rows", C.c_int32 * MG_MAX_LEVELS),
+                ("nnzb", C.c_int32 * MG_MAX_LEVELS), ("nf", C.c_int32), ("fine_n_rows", C.c_int32),
+                ("fine_nnzb", C.c_int32), ("pad0", C.c_int32), ("workspace", C.c_void_p)]
+
+
 class Adjoint(C.Structure):
     _fields_ = [("x", C.c_void_p), ("lp", C.c_void_p), ("F", C.c_void_p), ("b", C.c_void_p), ("E", C.c_void_p)]
 
@@ -99,6 +108,10 @@ SIGNATURES = {
     "gw_krylov_static_max_unknowns": (I64, []),
     "gw_bsr_krylov_solve_static": (C.c_int, [C.POINTER(Bsr), I32, I32, I32, P, P, C.c_double, I32, PI32, PD, P]),
     "gw_gmres_workspace_bytes": (I64, [I32, I32, I32]),
+    "gw_gmres_mg_workspace_bytes": (I64, [C.POINTER(Grid), I32, I32, I32]),
+    "gw_mg_plan_build": (C.c_int, [C.POINTER(Grid), C.POINTER(Bsr), P, I64, C.POINTER(MgPlan), P]),
+    "gw_bsr_gmres_mg_solve": (C.c_int, [C.POINTER(Grid), C.POINTER(Bsr), I32, C.POINTER(MgPlan), P, P, C.c_double, I32,
+                                        I32, P, I64, PI32, PD, P]),
     "gw_bsr_gmres_solve": (C.c_int, [C.POINTER(Bsr), I32, I32, P, P, C.c_double, I32, I32, P, PI32, PD, P]),
     "gw_bsr_spmv": (C.c_int, [C.POINTER(Bsr), I32, P, P, P]),
     "gw_bsr_spmv_t": (C.c_int, [C.POINTER(Bsr), I32, P, P, P]),
@@ -107,6 +120,7 @@ SIGNATURES = {
     "gw_g2p": (C.c_int, [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Particles), P, P, P]),
     "gw_return_map": (C.c_int, [C.POINTER(Material), I32, P, P, P, P, P, P, P, P]),
     "gw_profile_enable": (C.c_int, [I32]),
+    "gw_profile_count": (C.c_int, []),
     "gw_launch_count": (I64, []),
     "gw_profile_reset": (C.c_int, []),
     "gw_profile_read": (C.c_int, [I32, PD, C.POINTER(C.c_int64), PD]),

@@ -92,7 +92,6 @@ class LoadStepAdjoint:
         if ck is None:
             ck = self.tape.pop()
         e = self.e
-        lib = L.load()
         saved = self._swap(ck)
         try:
             # rebuild the step's active set and pattern from the checkpoint
@@ -119,14 +118,10 @@ class LoadStepAdjoint:
             AT = e.bsr_struct()
             AT.vals = _p(self._AT)
             self._lam[:n].zero_()
-            ws = e._kry_ws.get(lib.gw_gmres_workspace_bytes(e.n_rows, e.nf, e.restart))
-            it, rr = C.c_int32(0), C.c_double(0.0)
-            rc = lib.gw_bsr_gmres_solve(C.byref(AT), e.prec, e.precond, _p(self._ubar), _p(self._lam),
-                                        rtol if rtol is not None else e.krylov_rtol, e.krylov_max_iter, e.restart,
-                                        _p(ws), C.byref(it), C.byref(rr), s)
+            it, rr, rc = e.gmres_solve(AT, self._ubar, self._lam, rtol if rtol is not None else e.krylov_rtol)
             if rc not in (L.GW_OK, L.GW_ENOCONV):
                 L.check(rc, "adjoint transpose solve")
-            self.last_krylov = (it.value, rr.value)
+            self.last_krylov = (it, rr)
             L.call("gw_adjoint_residual", C.byref(g), C.byref(self.s._mat), C.byref(st), C.byref(pt), _p(e.u_new),
                    _p(e.u_old), _p(e.free_mask), C.byref(A), _p(self._lam), C.byref(q), s)
         finally:

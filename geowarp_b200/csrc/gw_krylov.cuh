@@ -613,11 +613,18 @@ __global__ void k_gm_dots(GmresVecs G, int pass) {
     __syncthreads();
     if (!last) return;
     __threadfence();
-    for (int i = threadIdx.x; i <= k; i += blockDim.x) {
+    // one warp per basis vector: lanes take the block partials in a fixed
+    // stride, then a fixed shuffle tree (deterministic)
+    for (int i = warp; i <= k; i += nwarp) {
         double s = 0.0;
-        for (int bb = 0; bb < (int)gridDim.x; ++bb) s += ((volatile double *)G.partials)[(size_t)bb * (kGmresMaxRestart + 1) + i];
-        if (pass == 0) G.sc->H[i][k] = s;
-        else G.sc->h2[i] = s;
+        for (int bb = lane; bb < (int)gridDim.x; bb += 32)
+            s += ((volatile double *)G.partials)[(size_t)bb * (kGmresMaxRestart + 1) + i];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) {
+            if (pass == 0) G.sc->H[i][k] = s;
+            else G.sc->h2[i] = s;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) G.sc->ticket = 0u;

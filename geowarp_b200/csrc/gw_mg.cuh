@@ -1,0 +1,512 @@
+// Geometric multigrid preconditioner on the background-grid node lattice.
+//
+// The reference solves each Newton correction with Warp's BiCGSTAB and a
+// diagonal preconditioner, or hands it to pyamg / SciPy on the host
+// (solvers/quasi_static_solver_2d.py:236-256).  Here the Krylov method is a
+// flexible GMRES whose preconditioner is one V-cycle over a hierarchy built
+// from the block-CSR Jacobian itself:
+//
+//   level l+1 lattice: node I sits on fine node 2I (per axis); a fine node with
+//     an even coordinate has one parent (weight 1), an odd one two (1/2 each);
+//     P is the tensor product of these weights, per field, zero on fixed DOFs;
+//   coarse operator: Galerkin A_{l+1} = P^T A_l P in the same 5^D-stencil
+//     block-CSR layout (a coarse block (I,J) gathers the fine blocks (i,j) of
+//     I's and J's children in a fixed order: deterministic, no atomics);
+//   smoother: damped node-block Jacobi; coarsest level (at most 40 unknowns):
+//     explicit dense inverse.
+//
+// Fixed (Dirichlet) DOFs are recognised from the Jacobian: their rows are
+// identity rows (the assembly writes 1 on the diagonal and nothing else).
+#pragma once
+#include "gw_krylov.cuh"
+
+namespace gw {
+
+constexpr int kMgMaxLevels = GW_MG_MAX_LEVELS;
+constexpr int kMgCoarseMax = 40;  // unknowns of the coarsest (dense) level
+
+// lattice node counts of a grid (cells + 1 per axis; 1 on unused axes)
+struct Lat {
+    int dim, n[3];
+};
+__host__ __device__ inline Lat lat_of(const gw_grid_t &g) {
+    Lat L;
+    L.dim = g.dim;
+    for (int k = 0; k < 3; ++k) L.n[k] = k < g.dim ? g.n_grid[k] + 1 : 1;
+    return L;
+}
+__device__ __forceinline__ void lat_coords(const Lat &L, int id, int c[3]) {
+    c[0] = id % L.n[0];
+    const int t = id / L.n[0];
+    c[1] = t % L.n[1];
+    c[2] = t / L.n[1];
+}
+__device__ __forceinline__ int lat_id(const Lat &L, const int c[3]) { return c[0] + L.n[0] * (c[1] + L.n[1] * c[2]); }
+
+// 1D prolongation weight of fine coordinate f below coarse coordinate C
+__device__ __forceinline__ double p_weight(int f, int C) {
+    const int d = f - 2 * C;
+    return d == 0 ? 1.0 : ((d == 1 || d == -1) ? 0.5 : 0.0);
+}
+
+// ---------------------------------------------------------------- fixed-DOF mask
+// bit f of fixed[r]: row (r, f) of A is an identity row
+template <int NF, typename VT>
+__global__ void k_mg_fixed_mask(PtrsA A, uint8_t *__restrict__ fixed) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n_rows) return;
+    const VT *vals = (const VT *)A.vals;
+    uint8_t m = 0;
+    for (int f = 0; f < NF; ++f) {
+        bool id = true;
+        bool diag_one = false;
+        for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1] && id; ++j) {
+            const VT *blk = vals + (size_t)j * NF * NF + f * NF;
+            const bool self = A.cols[j] == r;
+            for (int g = 0; g < NF; ++g) {
+                const double v = (double)blk[g];
+                if (self && g == f) diag_one = (v == 1.0);
+                else if (v != 0.0) { id = false; break; }
+            }
+        }
+        if (id && diag_one) m |= (uint8_t)(1u << f);
+    }
+    fixed[r] = m;
+}
+
+// ---------------------------------------------------------------- coarse active set
+__global__ void k_mg_coarse_flags(Lat Lf, PtrsA Af, Lat Lc, uint8_t *__restrict__ cflag) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= Af.n_rows) return;
+    int c[3];
+    lat_coords(Lf, Af.row2node[r], c);
+    int lo[3], cnt[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = c[k] >> 1;
+        cnt[k] = (k < Lf.dim && (c[k] & 1)) ? 2 : 1;
+    }
+    for (int a = 0; a < cnt[0]; ++a)
+        for (int b = 0; b < cnt[1]; ++b)
+            for (int d = 0; d < cnt[2]; ++d) {
+                const int C[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
+                cflag[lat_id(Lc, C)] = 1;
+            }
+}
+
+// coarse stencil mask of every coarse row and its block count
+template <int D>
+__global__ void k_mg_coarse_stencil(Lat Lf, PtrsA Af, Lat Lc, int nc_rows, const int *__restrict__ c_row2node,
+                                    uint32_t *__restrict__ c_stencil, int mw, int *__restrict__ c_count) {
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= nc_rows) return;
+    const int I = c_row2node[R];
+    int C[3];
+    lat_coords(Lc, I, C);
+    uint32_t mask[4] = {0u, 0u, 0u, 0u};
+    for (int oz = (D == 3 ? -1 : 0); oz <= (D == 3 ? 1 : 0); ++oz)
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                const int ci[3] = {2 * C[0] + ox, 2 * C[1] + oy, 2 * C[2] + oz};
+                bool in = true;
+                for (int k = 0; k < D; ++k) in = in && ci[k] >= 0 && ci[k] < Lf.n[k];
+                if (!in) continue;
+                const int i = lat_id(Lf, ci);
+                if (Af.node2row[i] < 0) continue;
+                for (int w = 0; w < mw; ++w) {
+                    uint32_t m = Af.stencil[(size_t)i * mw + w];
+                    while (m) {
+                        int bit = w * 32 + __ffs(m) - 1;
+                        m &= m - 1u;
+                        int cj[3] = {ci[0], ci[1], ci[2]};
+                        for (int k = 0; k < D; ++k) {
+                            cj[k] += bit % 5 - 2;
+                            bit /= 5;
+                        }
+                        // parents of fine node j, relative to C (always within [-2, 2])
+                        int lo[3], cnt[3];
+                        for (int k = 0; k < 3; ++k) {
+                            lo[k] = (cj[k] >> 1) - C[k];
+                            cnt[k] = (k < D && (cj[k] & 1)) ? 2 : 1;
+                        }
+                        for (int a = 0; a < cnt[0]; ++a)
+                            for (int b = 0; b < cnt[1]; ++b)
+                                for (int d = 0; d < cnt[2]; ++d) {
+                                    const int off[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
+                                    const int ob = offset_bit<D>(off);
+                                    mask[ob >> 5] |= 1u << (ob & 31);
+                                }
+                    }
+                }
+            }
+    int n = 0;
+    for (int w = 0; w < mw; ++w) {
+        c_stencil[(size_t)I * mw + w] = mask[w];
+        n += __popc(mask[w]);
+    }
+    c_count[R] = n;
+}
+
+// block -> row map of a block-CSR (for one-thread-per-block kernels)
+__global__ void k_mg_blockrow(const int *__restrict__ row_ptr, int n_rows, int *__restrict__ blockrow) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    for (int j = row_ptr[r]; j < row_ptr[r + 1]; ++j) blockrow[j] = r;
+}
+
+// ---------------------------------------------------------------- Galerkin product
+// One thread per coarse block (I, J): sum over children i of I and j of J,
+// in lattice order, of w_i w_j A(i, j) restricted to free DOFs.
+template <int D, int NF, typename VT>
+__global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, Lat Lc, PtrsA Ac,
+                         const int *__restrict__ c_blockrow) {
+    const int jb = blockIdx.x * blockDim.x + threadIdx.x;
+    if (jb >= Ac.nnzb) return;
+    const int R = c_blockrow[jb];
+    const int I = Ac.row2node[R], J = Ac.row2node[Ac.cols[jb]];
+    int CI[3], CJ[3];
+    lat_coords(Lc, I, CI);
+    lat_coords(Lc, J, CJ);
+    double acc[NF][NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int g = 0; g < NF; ++g) acc[f][g] = 0.0;
+    const VT *vals = (const VT *)Af.vals;
+    for (int iz = (D == 3 ? -1 : 0); iz <= (D == 3 ? 1 : 0); ++iz)
+        for (int iy = -1; iy <= 1; ++iy)
+            for (int ix = -1; ix <= 1; ++ix) {
+                const int ci[3] = {2 * CI[0] + ix, 2 * CI[1] + iy, 2 * CI[2] + iz};
+                bool in = true;
+                for (int k = 0; k < D; ++k) in = in && ci[k] >= 0 && ci[k] < Lf.n[k];
+                if (!in) continue;
+                const int i = lat_id(Lf, ci);
+                const int fr = Af.node2row[i];
+                if (fr < 0) continue;
+                double wi = 1.0;
+                for (int k = 0; k < D; ++k) wi *= p_weight(ci[k], CI[k]);
+                const uint8_t fi = ffixed[fr];
+                for (int jz = (D == 3 ? -1 : 0); jz <= (D == 3 ? 1 : 0); ++jz)
+                    for (int jy = -1; jy <= 1; ++jy)
+                        for (int jx = -1; jx <= 1; ++jx) {
+                            const int cj[3] = {2 * CJ[0] + jx, 2 * CJ[1] + jy, 2 * CJ[2] + jz};
+                            int off[3] = {0, 0, 0};
+                            bool ok = true;
+                            for (int k = 0; k < D; ++k) {
+                                off[k] = cj[k] - ci[k];
+                                ok = ok && off[k] >= -2 && off[k] <= 2 && cj[k] >= 0 && cj[k] < Lf.n[k];
+                            }
+                            if (!ok) continue;
+                            const int slot = stencil_slot(Af.stencil, Af.mw, i, offset_bit<D>(off));
+                            if (slot < 0) continue;
+                            const int fc = Af.node2row[lat_id(Lf, cj)];
+                            if (fc < 0) continue;
+                            double wj = 1.0;
+                            for (int k = 0; k < D; ++k) wj *= p_weight(cj[k], CJ[k]);
+                            const uint8_t fj = ffixed[fc];
+                            const VT *blk = vals + ((size_t)Af.row_ptr[fr] + slot) * NF * NF;
+                            const double w = wi * wj;
+#pragma unroll
+                            for (int f = 0; f < NF; ++f) {
+                                if ((fi >> f) & 1) continue;
+#pragma unroll
+                                for (int g = 0; g < NF; ++g)
+                                    if (!((fj >> g) & 1)) acc[f][g] += w * (double)blk[f * NF + g];
+                            }
+                        }
+            }
+    double *out = (double *)Ac.vals + (size_t)jb * NF * NF;
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+#pragma unroll
+        for (int g = 0; g < NF; ++g) out[f * NF + g] = acc[f][g];
+}
+
+// coarse rows that received nothing (every child DOF fixed) become identity rows
+template <int NF>
+__global__ void k_mg_fix_empty_rows(PtrsA A) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n_rows) return;
+    double *vals = (double *)A.vals;
+    int self = -1;
+    for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1]; ++j)
+        if (A.cols[j] == r) self = j;
+    if (self < 0) return;
+    for (int f = 0; f < NF; ++f) {
+        bool empty = true;
+        for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1] && empty; ++j)
+            for (int g = 0; g < NF; ++g)
+                if (vals[(size_t)j * NF * NF + f * NF + g] != 0.0) { empty = false; break; }
+        if (empty) vals[(size_t)self * NF * NF + f * NF + f] = 1.0;
+    }
+}
+
+// ---------------------------------------------------------------- cycle kernels
+// x_out = x_in + omega Minv (b - A x_in); zero_init: x_in = 0 (x_out = omega Minv b)
+template <int NF, typename VT>
+__global__ void k_mg_jacobi(PtrsA A, const double *__restrict__ Minv, const double *__restrict__ b,
+                            const double *__restrict__ x_in, double *__restrict__ x_out, double omega, int zero_init,
+                            const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    if (zero_init) {
+        for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < A.n_rows; r += gridDim.x * blockDim.x) {
+            double t[NF], z[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) t[f] = b[(size_t)r * NF + f];
+            apply_minv<NF>(Minv, r, t, z);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) x_out[(size_t)r * NF + f] = omega * z[f];
+        }
+        return;
+    }
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+        double acc[NF];
+        row_mv<NF, VT>(A, r, x_in, acc);
+        if ((threadIdx.x & 31) == 0) {
+            double t[NF], z[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) t[f] = b[(size_t)r * NF + f] - acc[f];
+            apply_minv<NF>(Minv, r, t, z);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) x_out[(size_t)r * NF + f] = x_in[(size_t)r * NF + f] + omega * z[f];
+        }
+    }
+}
+
+// r = b - A x
+template <int NF, typename VT>
+__global__ void k_mg_residual(PtrsA A, const double *__restrict__ b, const double *__restrict__ x,
+                              double *__restrict__ r_out, const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+        double acc[NF];
+        row_mv<NF, VT>(A, r, x, acc);
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) r_out[(size_t)r * NF + f] = b[(size_t)r * NF + f] - acc[f];
+    }
+}
+
+// b_c = P^T r_f
+template <int D, int NF>
+__global__ void k_mg_restrict(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, Lat Lc, PtrsA Ac,
+                              const double *__restrict__ rf, double *__restrict__ bc, const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= Ac.n_rows) return;
+    int C[3];
+    lat_coords(Lc, Ac.row2node[R], C);
+    double acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[f] = 0.0;
+    for (int oz = (D == 3 ? -1 : 0); oz <= (D == 3 ? 1 : 0); ++oz)
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox) {
+                const int ci[3] = {2 * C[0] + ox, 2 * C[1] + oy, 2 * C[2] + oz};
+                bool in = true;
+                for (int k = 0; k < D; ++k) in = in && ci[k] >= 0 && ci[k] < Lf.n[k];
+                if (!in) continue;
+                const int fr = Af.node2row[lat_id(Lf, ci)];
+                if (fr < 0) continue;
+                double w = 1.0;
+                for (int k = 0; k < D; ++k) w *= p_weight(ci[k], C[k]);
+                const uint8_t fx = ffixed[fr];
+#pragma unroll
+                for (int f = 0; f < NF; ++f)
+                    if (!((fx >> f) & 1)) acc[f] += w * rf[(size_t)fr * NF + f];
+            }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) bc[(size_t)R * NF + f] = acc[f];
+}
+
+// x_f += P x_c
+template <int D, int NF>
+__global__ void k_mg_prolong(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, Lat Lc, PtrsA Ac,
+                             const double *__restrict__ xc, double *__restrict__ xf, const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= Af.n_rows) return;
+    int c[3];
+    lat_coords(Lf, Af.row2node[r], c);
+    int lo[3], cnt[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = c[k] >> 1;
+        cnt[k] = (k < D && (c[k] & 1)) ? 2 : 1;
+    }
+    double acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[f] = 0.0;
+    for (int a = 0; a < cnt[0]; ++a)
+        for (int b = 0; b < cnt[1]; ++b)
+            for (int d = 0; d < cnt[2]; ++d) {
+                const int C[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
+                const int R = Ac.node2row[lat_id(Lc, C)];
+                if (R < 0) continue;
+                double w = 1.0;
+                for (int k = 0; k < D; ++k) w *= p_weight(c[k], C[k]);
+#pragma unroll
+                for (int f = 0; f < NF; ++f) acc[f] += w * xc[(size_t)R * NF + f];
+            }
+    const uint8_t fx = ffixed[r];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+        if (!((fx >> f) & 1)) xf[(size_t)r * NF + f] += acc[f];
+}
+
+// ---------------------------------------------------------------- coarsest level
+// dense row-major copy of a block-CSR matrix (M zeroed by the caller)
+template <int NF, typename VT>
+__global__ void k_mg_dense_build(PtrsA A, double *__restrict__ M, int n) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n_rows) return;
+    const VT *vals = (const VT *)A.vals;
+    for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1]; ++j) {
+        const int c = A.cols[j];
+        for (int f = 0; f < NF; ++f)
+            for (int g = 0; g < NF; ++g)
+                M[(size_t)(r * NF + f) * n + c * NF + g] = (double)vals[(size_t)j * NF * NF + f * NF + g];
+    }
+}
+
+// Inverse of the coarsest operator by in-place Gauss-Jordan elimination with
+// partial pivoting, one CTA, the matrix held in dynamic shared memory
+// (n <= kMgCoarseMax, n*n doubles).  Step k: swap the pivot row into place,
+// divide row k by the pivot p (a_kk := 1/p), and for every other row i with
+// f = a_ik subtract f * row k (a_ik := -f/p).  The row interchanges are undone
+// at the end by swapping columns in reverse order.  A zero pivot column is
+// replaced by a unit pivot, so a singular coarse operator weakens the
+// preconditioner instead of producing non-finite values.  Pivot ties go to the
+// lowest row: the result is deterministic.
+__global__ void k_mg_dense_invert(const double *__restrict__ M, double *__restrict__ Inv, int n) {
+    extern __shared__ double a[];
+    __shared__ int perm[kMgCoarseMax];
+    __shared__ double fk[kMgCoarseMax];
+    __shared__ int piv_s;
+    __shared__ double red_v[32];
+    __shared__ int red_i[32];
+    const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
+    for (int q = t; q < n * n; q += nt) a[q] = M[q];
+    __syncthreads();
+    for (int k = 0; k < n; ++k) {
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + t; i < n; i += nt) {
+            const double v = fabs(a[i * n + k]);
+            if (v > best) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ov = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+        }
+        if (lane == 0) { red_v[w] = best; red_i[w] = bi; }
+        __syncthreads();
+        if (t == 0) {
+            double bv = red_v[0];
+            int b = red_i[0];
+            for (int q = 1; q < (nt >> 5); ++q)
+                if (red_v[q] > bv || (red_v[q] == bv && red_i[q] < b)) { bv = red_v[q]; b = red_i[q]; }
+            if (!(bv > 0.0)) {  // no nonzero pivot: unit pivot in place
+                a[k * n + k] = 1.0;
+                b = k;
+            }
+            piv_s = b;
+            perm[k] = b;
+        }
+        __syncthreads();
+        const int p = piv_s;
+        if (p != k)
+            for (int j = t; j < n; j += nt) {
+                const double tmp = a[k * n + j];
+                a[k * n + j] = a[p * n + j];
+                a[p * n + j] = tmp;
+            }
+        __syncthreads();
+        const double pinv = 1.0 / a[k * n + k];
+        for (int i = t; i < n; i += nt) fk[i] = a[i * n + k];
+        __syncthreads();
+        for (int j = t; j < n; j += nt) a[k * n + j] = (j == k) ? pinv : a[k * n + j] * pinv;
+        __syncthreads();
+        for (int q = t; q < n * n; q += nt) {
+            const int i = q / n, j = q - (q / n) * n;
+            if (i == k) continue;
+            const double f = fk[i];
+            if (j == k) a[q] = -f * pinv;
+            else if (f != 0.0) a[q] -= f * a[k * n + j];
+        }
+        __syncthreads();
+    }
+    // undo the row interchanges as column interchanges, last first
+    for (int k = n - 1; k >= 0; --k) {
+        const int p = perm[k];
+        if (p != k)
+            for (int i = t; i < n; i += nt) {
+                const double tmp = a[i * n + k];
+                a[i * n + k] = a[i * n + p];
+                a[i * n + p] = tmp;
+            }
+        __syncthreads();
+    }
+    for (int q = t; q < n * n; q += nt) Inv[q] = a[q];
+}
+
+// x = Inv b (one warp per row)
+__global__ void k_mg_dense_apply(const double *__restrict__ Inv, const double *__restrict__ b, double *__restrict__ x,
+                                 int n, const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int lane = threadIdx.x & 31;
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += nw) {
+        double s = 0.0;
+        for (int j = lane; j < n; j += 32) s += Inv[(size_t)i * n + j] * b[j];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) x[i] = s;
+    }
+}
+
+// ---------------------------------------------------------------- flexible GMRES glue
+// v_k = w / s -> V[k] and the cycle's right-hand side
+__global__ void k_gm_next_flex(size_t n, GmresVecs G, int start, double *__restrict__ mg_b) {
+    if (G.sc->cycle_done) return;
+    const int k = G.sc->k;
+    const double ih = 1.0 / (start ? G.sc->beta : G.sc->wnorm);
+    double *vn = G.V + (size_t)k * G.n;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        const double v = G.w[q] * ih;
+        vn[q] = v;
+        mg_b[q] = v;
+    }
+}
+
+// w = A z_k, and z_k -> Z[k] (z is the V-cycle's output)
+template <int NF, typename VT>
+__global__ void k_gm_spmv_keep(PtrsA A, GmresVecs G, double *__restrict__ Z) {
+    if (G.sc->cycle_done) return;
+    double *zk = Z + (size_t)G.sc->k * G.n;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+        double acc[NF];
+        row_mv<NF, VT>(A, r, G.z, acc);
+        if ((threadIdx.x & 31) == 0)
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                G.w[(size_t)r * NF + f] = acc[f];
+                zk[(size_t)r * NF + f] = G.z[(size_t)r * NF + f];
+            }
+    }
+}
+
+// x += Z y
+__global__ void k_gm_update_x_flex(size_t n, GmresVecs G, const double *__restrict__ Z) {
+    const GScalars *sc = G.sc;
+    if (sc->done) return;
+    const int k = sc->k;
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int i = 0; i < k; ++i) s += sc->y[i] * Z[(size_t)i * n + q];
+        G.x[q] += s;
+    }
+}
+
+}  // namespace gw

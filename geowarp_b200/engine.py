@@ -32,7 +32,7 @@ MODEL_IDS = {
 }
 
 PRECISIONS = {"fp64": L.PREC_F64, "mixed": L.PREC_F32}
-PRECONDS = {"diag": L.PRECOND_DIAG, "block": L.PRECOND_BLOCK}
+PRECONDS = {"diag": L.PRECOND_DIAG, "block": L.PRECOND_BLOCK, "mg": "mg"}
 
 
 def _p(t):
@@ -91,8 +91,8 @@ class Engine:
     KINDS = {"solid2d": L.KIND_SOLID2D, "coupled2d": L.KIND_COUPLED2D, "coupled3d": L.KIND_COUPLED3D}
 
     def __init__(self, kind, n_grid, h, h_nodes, domain_min, domain_max, x_init, device=None,
-                 precision="fp64", precond="block", krylov_rtol=None, krylov_max_iter=20000, krylov="gmres",
-                 restart=100):
+                 precision="fp64", precond="mg", krylov_rtol=None, krylov_max_iter=20000, krylov="gmres",
+                 restart=None):
         if not torch.cuda.is_available():
             raise RuntimeError("geowarp_b200 needs a CUDA device (there is no CPU fallback)")
         L.load()
@@ -116,7 +116,9 @@ class Engine:
         if krylov not in ("gmres", "bicgstab"):
             raise ValueError(f"unknown Krylov method {krylov!r}")
         self.krylov_method = krylov
-        self.restart = int(restart)
+        # flexible GMRES with a V-cycle needs few iterations; the Jacobi-preconditioned
+        # one needs a long basis
+        self.restart = int(restart) if restart is not None else (30 if precond == "mg" else 100)
         self.mw = 1 if self.D == 2 else 4
 
         dev = self.device
@@ -164,6 +166,7 @@ class Engine:
         self._vals = _Buf(dev)
         self._R = torch.zeros(1, **f64)
         self._delta = torch.zeros(1, **f64)
+        self._mg_plan = None
         # consistent-mass system (u-p kinds)
         if self.nf > self.D:
             self.touched = torch.zeros(nn, dtype=torch.uint8, device=dev)
@@ -249,6 +252,7 @@ class Engine:
 
     def build_system(self):
         """Row compaction and block-CSR pattern, once per load step."""
+        self._mg_plan = None  # the multigrid plan follows the pattern
         g, s = self.grid_struct(), self.stream
         nr = C.c_int32(0)
         L.call("gw_compact_rows", C.byref(g), _p(self.node_active), _p(self.boundary), _p(self.node2row),
@@ -360,10 +364,9 @@ class Engine:
         it, rr = C.c_int32(0), C.c_double(0.0)
         rtol = rtol if rtol is not None else self.krylov_rtol
         if self.krylov_method == "gmres":
-            ws = self._kry_ws.get(lib.gw_gmres_workspace_bytes(self.n_rows, self.nf, self.restart))
-            rc = lib.gw_bsr_gmres_solve(C.byref(A), self.prec, self.precond, _p(self._R), _p(self._delta), rtol,
-                                        self.krylov_max_iter, self.restart, _p(ws), C.byref(it), C.byref(rr),
-                                        self.stream)
+            return self.gmres_solve(A, self._R, self._delta, rtol)
+        if self.precond == "mg":
+            raise ValueError("the multigrid preconditioner runs inside GMRES (krylov='gmres')")
         else:
             ws = self._kry_ws.get(lib.gw_krylov_workspace_bytes(self.n_rows, self.nf, self.prec))
             rc = lib.gw_bsr_krylov_solve(C.byref(A), self.prec, L.KRYLOV_BICGSTAB, self.precond, _p(self._R),
@@ -371,6 +374,34 @@ class Engine:
                                          C.byref(rr), self.stream)
         if rc not in (L.GW_OK, L.GW_ENOCONV, L.GW_EBREAKDOWN):
             L.check(rc, "Krylov")
+        return it.value, rr.value, rc
+
+    def gmres_solve(self, A, b, x, rtol):
+        """GMRES on block-CSR A (rows of this engine's active set): node-block /
+        diagonal Jacobi (gw_bsr_gmres_solve) or a geometric-multigrid V-cycle
+        on the background grid (gw_bsr_gmres_mg_solve)."""
+        lib = L.load()
+        it, rr = C.c_int32(0), C.c_double(0.0)
+        if self.precond == "mg":
+            g = self.grid_struct()
+            nbytes = lib.gw_gmres_mg_workspace_bytes(C.byref(g), self.n_rows, self.nf, self.restart)
+            ws = self._kry_ws.get(nbytes)
+            plan = self._mg_plan
+            if plan is None or plan.workspace != ws.data_ptr() or plan.fine_nnzb != A.nnzb:
+                # coarse patterns: once per load step (the pattern is fixed within it)
+                plan = L.MgPlan()
+                L.call("gw_mg_plan_build", C.byref(g), C.byref(A), _p(ws), ws.numel(), C.byref(plan), self.stream)
+                self._mg_plan = plan
+            rc = lib.gw_bsr_gmres_mg_solve(C.byref(g), C.byref(A), self.prec, C.byref(plan), _p(b), _p(x), rtol,
+                                           self.krylov_max_iter, self.restart, _p(ws), ws.numel(), C.byref(it),
+                                           C.byref(rr), self.stream)
+        else:
+            ws = self._kry_ws.get(lib.gw_gmres_workspace_bytes(self.n_rows, self.nf, self.restart))
+            rc = lib.gw_bsr_gmres_solve(C.byref(A), self.prec, self.precond, _p(b), _p(x), rtol,
+                                        self.krylov_max_iter, self.restart, _p(ws), C.byref(it), C.byref(rr),
+                                        self.stream)
+        if rc not in (L.GW_OK, L.GW_ENOCONV, L.GW_EBREAKDOWN):
+            L.check(rc, "GMRES")
         return it.value, rr.value, rc
 
     def apply_increment(self):

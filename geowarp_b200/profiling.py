@@ -4,8 +4,6 @@ import ctypes as C
 
 from . import _lib as L
 
-N_CLASSES = 8
-
 
 @contextlib.contextmanager
 def kernel_timer():
@@ -17,7 +15,7 @@ def kernel_timer():
         yield rec
     finally:
         lib.gw_profile_enable(0)
-        for c in range(N_CLASSES):
+        for c in range(lib.gw_profile_count()):
             ms, n, b = C.c_double(0), C.c_int64(0), C.c_double(0)
             L.check(lib.gw_profile_read(c, C.byref(ms), C.byref(n), C.byref(b)), "gw_profile_read")
             rec[lib.gw_profile_name(c).decode()] = dict(ms=ms.value, launches=n.value, bytes=b.value)

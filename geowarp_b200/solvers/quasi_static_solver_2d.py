@@ -43,7 +43,7 @@ class DofStruct:
 
 class quasi_static_solver_2d:
     def __init__(self, background_grid_dict, particles_dict, iteration_dict, material_dict, load_dict,
-                 precision="fp64", device=None, precond="block"):
+                 precision="fp64", device=None, precond="mg"):
         g = background_grid_dict
         self.n_grid_x = g["n_grid_x"]
         self.n_grid_y = g["n_grid_y"]

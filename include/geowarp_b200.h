@@ -269,6 +269,42 @@ int64_t gw_gmres_workspace_bytes(int32_t n_rows, int32_t nf, int32_t restart);
 int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const double *b, double *x, double rtol,
                        int32_t max_iter, int32_t restart, void *workspace, int32_t *iters_host, double *relres_host,
                        void *stream);
+/* Flexible GMRES(restart) preconditioned by one geometric-multigrid V-cycle on
+ * the background-grid node lattice of `grid` (the grid whose node ids A's
+ * row2node/node2row/stencil use).  Replaces the same solver choices as
+ * gw_bsr_gmres_solve (solvers/quasi_static_solver_2d.py:236-256; the
+ * reference's host pyamg path is the closest counterpart).  Hierarchy:
+ * factor-2 coarsening per axis, Galerkin coarse operators P^T A P in the same
+ * block-CSR layout (FP64), two damped node-block-Jacobi sweeps before and after
+ * each coarse correction, an explicit dense inverse on the coarsest level
+ * (<= 40 unknowns).  Identity rows of A (Dirichlet DOFs) are excluded from the
+ * transfer operators.
+ *
+ * gw_mg_plan_build: the pattern phase (coarse active sets, stencils, block-CSR
+ * patterns), written into the workspace, with the level sizes returned in the
+ * host struct *plan_host.  It reads A's pattern only and synchronises twice per
+ * coarse level.  A plan stays valid while A keeps its pattern (one load step,
+ * and the transpose of its Jacobian, whose pattern is the same) and the same
+ * workspace is passed.
+ * gw_bsr_gmres_mg_solve: the numeric phase (Galerkin values, smoothers, dense
+ * inverse; no host reads) and the solve.  plan_host == NULL builds a plan
+ * first.  workspace: at least gw_gmres_mg_workspace_bytes(grid, n_rows, nf,
+ * restart) bytes (the plan needs the hierarchy part, which comes first). */
+#define GW_MG_MAX_LEVELS 20
+typedef struct gw_mg_plan {
+    int32_t levels;                     /* levels holding a matrix; the last one is solved densely */
+    int32_t dense_n;                    /* unknowns of the coarsest level                          */
+    int32_t n_rows[GW_MG_MAX_LEVELS];
+    int32_t nnzb[GW_MG_MAX_LEVELS];
+    int32_t nf, fine_n_rows, fine_nnzb, pad0;
+    const void *workspace;              /* the coarse patterns live in this workspace              */
+} gw_mg_plan_t;
+int64_t gw_gmres_mg_workspace_bytes(const gw_grid_t *grid, int32_t n_rows, int32_t nf, int32_t restart);
+int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *workspace, int64_t workspace_bytes,
+                     gw_mg_plan_t *plan_host, void *stream);
+int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, const gw_mg_plan_t *plan_host,
+                          const double *b, double *x, double rtol, int32_t max_iter, int32_t restart, void *workspace,
+                          int64_t workspace_bytes, int32_t *iters_host, double *relres_host, void *stream);
 /* y = A x (x, y FP64 of length n_rows*nf; A values in prec). */
 int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream);
 /* y = A^T x. */
@@ -325,10 +361,14 @@ int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *mat, const g
 
 /* ------------------------------------------------------------ kernel timing
  * Optional CUDA-event timing of the engine's main kernels (off by default):
- * classes 0..7 = k_assemble, k_gm_spmv, k_gm_dots, k_gm_update, k_gm_next,
- * k_g2p, k_adjoint_g2p, k_adjoint_residual.  gw_profile_read synchronises and
+ * classes 0..11 = k_assemble, k_gm_spmv, k_gm_dots, k_gm_update, k_gm_next,
+ * k_g2p, k_adjoint_g2p, k_adjoint_residual, k_mg_jacobi, k_mg_residual,
+ * k_mg_restrict/prolong, mg_setup (the whole hierarchy build, host reads
+ * included).  gw_profile_read synchronises and
  * returns the total time, launch count and algorithmic bytes of a class. */
 int gw_profile_enable(int32_t on);
+/* Number of timing classes (k_assemble ... mg_setup) gw_profile_read accepts. */
+int gw_profile_count(void);
 int gw_profile_reset(void);
 /* Number of kernels the library has launched since it was loaded (host
  * counter; no counterpart in the reference, which launches through Warp). */

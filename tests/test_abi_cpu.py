@@ -36,7 +36,8 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_c():
     from geowarp_b200 import _lib
     structs = {"gw_grid_t": _lib.Grid, "gw_material_t": _lib.Material, "gw_step_t": _lib.Step,
-               "gw_particles_t": _lib.Particles, "gw_bsr_t": _lib.Bsr}
+               "gw_particles_t": _lib.Particles, "gw_bsr_t": _lib.Bsr, "gw_adjoint_t": _lib.Adjoint,
+               "gw_mg_plan_t": _lib.MgPlan}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

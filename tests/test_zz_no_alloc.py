@@ -48,11 +48,11 @@ def _solve(e, static, rtol=1e-12):
     A = e.bsr_struct()
     it, rr = C.c_int32(0), C.c_double(0.0)
     if static:
-        rc = lib.gw_bsr_krylov_solve_static(C.byref(A), e.prec, L.KRYLOV_BICGSTAB, e.precond, _p(e._R), _p(x), rtol,
+        rc = lib.gw_bsr_krylov_solve_static(C.byref(A), e.prec, L.KRYLOV_BICGSTAB, L.PRECOND_BLOCK, _p(e._R), _p(x), rtol,
                                             20000, C.byref(it), C.byref(rr), e.stream)
     else:
         ws = torch.zeros(lib.gw_krylov_workspace_bytes(e.n_rows, e.nf, e.prec), dtype=torch.uint8, device=e.device)
-        rc = lib.gw_bsr_krylov_solve(C.byref(A), e.prec, L.KRYLOV_BICGSTAB, e.precond, _p(e._R), _p(x), rtol, 20000,
+        rc = lib.gw_bsr_krylov_solve(C.byref(A), e.prec, L.KRYLOV_BICGSTAB, L.PRECOND_BLOCK, _p(e._R), _p(x), rtol, 20000,
                                      _p(ws), C.byref(it), C.byref(rr), e.stream)
     torch.cuda.synchronize()
     return rc, x, it.value, rr.value
