@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geowarp", choices=["geowarp", "reference"])
     ap.add_argument("--small", action="store_true", help="64x32-cell variant for quick checks")
+    ap.add_argument("--workload", default="footing", choices=["footing", "batched"],
+                    help="footing: the strip footing (default); batched: 64 inverse-analysis blocks in one engine")
+    ap.add_argument("--instances", type=int, default=64, help="blocks of the batched workload")
     ap.add_argument("--profile", action="store_true", help="also time the dominant kernel (instrumented pass)")
     ap.add_argument("--ncu", action="store_true",
                     help="run warmup + steps load steps (fwd+adjoint, mixed) with no timing: the command profiled by ncu")
@@ -105,13 +108,85 @@ class ClockSampler:
                 "samples": len(rows)}
 
 
+# ------------------------------------------------------------------ workloads
+class FootingWorkload:
+    """The strip footing: one instance per load step."""
+
+    def __init__(self, args):
+        self.fk = footing_kwargs(args.small)
+        self.units = 1
+        self.n_steps = N_STEPS_TOTAL
+        self.config = dict(WORKLOAD)
+        self.metric = METRIC
+
+    def make(self, precision, dev):
+        from geowarp_b200 import problems
+        from geowarp_b200.adjoint import LoadStepAdjoint
+        s = problems.strip_footing_2d(precision=precision, device=dev, **self.fk)
+        return s, LoadStepAdjoint(s)
+
+    def seed(self, adj, k):
+        adj.seed_displacement_misfit()
+
+    def errors(self, s_mx, s_64):
+        return {"footing_force": abs(s_mx.footing_force - s_64.footing_force) / abs(s_64.footing_force)}
+
+
+class BatchedWorkload:
+    """Batched inverse analysis: n self-weight blocks (cell counts seeded
+    uniformly in 32x32..128x64, per-particle log E a Gaussian random field)
+    in one engine; each load step is forward + adjoint of the summed
+    displacement misfit to targets made by a second field."""
+
+    def __init__(self, args):
+        from geowarp_b200 import batch
+        self.n = args.instances
+        self.sizes = batch.instance_sizes(self.n, seed=0)
+        self.logE = batch.random_fields(self.sizes, seed=1000)
+        self.logE_target = batch.random_fields(self.sizes, seed=2000)
+        self.units = self.n
+        self.n_steps = 50
+        self.targets = None
+        npart = sum(a * b * 4 for a, b in self.sizes)
+        self.config = dict(workload=f"batched inverse analysis: {self.n} self-weight blocks in one engine",
+                           cells="per block uniform (seed 0) in 32x32..128x64, dx=0.05 m, shelf-packed with 4 empty "
+                                 "cells between blocks", particles=npart, ppc="2x2",
+                           material="Hencky elastic, nu=0.3, log E = Gaussian random field (mean ln 1e7, std 0.3, "
+                                    "correlation length 0.5 m, seeds 1000+q); targets from a second field (seeds 2000+q)",
+                           load="self-weight rho=2000 kg/m3 g=9.81 ramped over 50 load steps",
+                           units="value counts block load steps (blocks x load steps)")
+        self.metric = METRIC.replace("load steps/s", "block load steps/s")
+
+    def make(self, precision, dev):
+        from geowarp_b200.adjoint import LoadStepAdjoint
+        from geowarp_b200.batch import BatchedBlocks
+        bb = BatchedBlocks(self.sizes, logE=self.logE, precision=precision, device=dev)
+        return bb.solver, LoadStepAdjoint(bb.solver)
+
+    def prepare(self, n_steps_run, dev):
+        """Target displacement after each load step, from the target field."""
+        import torch
+        from geowarp_b200.batch import BatchedBlocks
+        bt = BatchedBlocks(self.sizes, logE=self.logE_target, precision="fp64", device=dev)
+        self.targets = []
+        for k in range(n_steps_run):
+            bt.solver.advance_one_step(k, self.n_steps)
+            self.targets.append(bt.displacement().clone())
+        del bt
+        torch.cuda.empty_cache()
+
+    def seed(self, adj, k):
+        adj.seed_displacement_misfit(self.targets[k])
+
+    def errors(self, s_mx, s_64):
+        return {}
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_geowarp(args):
     import torch
     import torch.distributed as dist
     from geowarp_b200 import _lib as L
-    from geowarp_b200 import problems
-    from geowarp_b200.adjoint import LoadStepAdjoint
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -120,8 +195,10 @@ def run_geowarp(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
     dev = torch.device("cuda", torch.cuda.current_device())
-    fk = footing_kwargs(args.small)
+    wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
     W, K = args.warmup, args.steps
+    if hasattr(wl, "prepare"):
+        wl.prepare(W + K + 1, dev)
     lib = L.load()
     # written between timed load steps: evicts the 126 MB L2 (256 MB memset, ~0.05 ms)
     l2_flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
@@ -131,18 +208,17 @@ def run_geowarp(args):
         if world > 1:
             dist.barrier()
 
-    def one_step(s, adj, k):
+    def one_step(adj, k):
         # forward load step (checkpointed), then its adjoint seeded with the
-        # displacement misfit of L = 1/2 |x - x0|^2
-        adj.forward_step(k, N_STEPS_TOTAL, keep=False)
-        adj.seed_displacement_misfit()
+        # displacement misfit
+        adj.forward_step(k, wl.n_steps, keep=False)
+        wl.seed(adj, k)
         adj.backward_step()
 
     # ---- mixed precision, resident (value)
-    s_mx = problems.strip_footing_2d(precision="mixed", device=dev, **fk)
-    adj_mx = LoadStepAdjoint(s_mx)
+    s_mx, adj_mx = wl.make("mixed", dev)
     for k in range(W):
-        one_step(s_mx, adj_mx, k)
+        one_step(adj_mx, k)
     sync()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as cs:
@@ -151,7 +227,7 @@ def run_geowarp(args):
         ev0.record()
         for k in range(W, W + K):
             l2_flush.zero_()
-            one_step(s_mx, adj_mx, k)
+            one_step(adj_mx, k)
         ev1.record()
         sync()
         launches = lib.gw_launch_count() - n_launch0
@@ -159,35 +235,37 @@ def run_geowarp(args):
     clocks = cs.summary()
 
     # ---- plain FP64 on the same steps (error reference and its own throughput)
-    s_64 = problems.strip_footing_2d(precision="fp64", device=dev, **fk)
-    adj_64 = LoadStepAdjoint(s_64)
+    s_64, adj_64 = wl.make("fp64", dev)
     for k in range(W):
-        one_step(s_64, adj_64, k)
+        one_step(adj_64, k)
     sync()
     ev0.record()
     for k in range(W, W + K):
         l2_flush.zero_()
-        one_step(s_64, adj_64, k)
+        one_step(adj_64, k)
     ev1.record()
     sync()
     ms_64 = ev0.elapsed_time(ev1)
     disp_mx = (s_mx.x_particles - s_mx.x0)
     disp_64 = (s_64.x_particles - s_64.x0)
-    rel_disp = float((disp_mx - disp_64).abs().max() / disp_64.abs().max())
-    rel_sig = float((s_mx.particle_Cauchy_stress_array - s_64.particle_Cauchy_stress_array).abs().max()
-                    / s_64.particle_Cauchy_stress_array.abs().max())
-    rel_grad = float((adj_mx.grad_E - adj_64.grad_E).abs().max() / adj_64.grad_E.abs().max().clamp_min(1e-300))
-    rel_force = abs(s_mx.footing_force - s_64.footing_force) / abs(s_64.footing_force)
+    errs = {"displacement": float((disp_mx - disp_64).abs().max() / disp_64.abs().max()),
+            "cauchy_stress": float((s_mx.particle_Cauchy_stress_array - s_64.particle_Cauchy_stress_array).abs().max()
+                                   / s_64.particle_Cauchy_stress_array.abs().max())}
+    errs.update(wl.errors(s_mx, s_64))
+    errs["grad_E"] = float((adj_mx.grad_E - adj_64.grad_E).abs().max() / adj_64.grad_E.abs().max().clamp_min(1e-300))
+    errs["norm"] = "max-abs difference / max-abs FP64 value"
+    newton = {"mixed_iters": newton_stats(s_mx.engine), "fp64_iters": newton_stats(s_64.engine)}
+    del s_64, adj_64
+    torch.cuda.empty_cache()
 
     # ---- end to end through the public API with the particle state held on the
     # host: every step copies the state in (pinned H2D), runs the load step and
     # its adjoint, and copies the new state, the stress and the gradient out
-    s_e2e = problems.strip_footing_2d(precision="mixed", device=dev, **fk)
-    adj_e2e = LoadStepAdjoint(s_e2e)
+    s_e2e, adj_e2e = wl.make("mixed", dev)
     e = s_e2e.engine
     state = ("x", "F_old", "b_old", "lp")
     for k in range(W):
-        one_step(s_e2e, adj_e2e, k)
+        one_step(adj_e2e, k)
     host = {name: torch.empty_like(getattr(e, name), device="cpu").pin_memory() for name in state}
     for name in state:
         host[name].copy_(getattr(e, name))
@@ -201,7 +279,7 @@ def run_geowarp(args):
         l2_flush.zero_()
         for name in state:
             getattr(e, name).copy_(host[name], non_blocking=True)
-        one_step(s_e2e, adj_e2e, k)
+        one_step(adj_e2e, k)
         for name in state:
             host[name].copy_(getattr(e, name), non_blocking=True)
         sigma_host.copy_(e.sigma, non_blocking=True)
@@ -210,37 +288,38 @@ def run_geowarp(args):
     ev1.record()
     sync()
     ms_e2e = ev0.elapsed_time(ev1)
+    del s_e2e, adj_e2e
+    torch.cuda.empty_cache()
 
     # ---- dominant kernel, instrumented pass on one more step (not part of value)
-    roof = roofline_pass(s_mx, adj_mx, W + K, fk, dev)
+    roof = roofline_pass(adj_mx, W + K, wl)
 
     vals = torch.tensor([ms_mx, ms_64, ms_e2e], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(vals, op=dist.ReduceOp.MAX)
     ms_mx, ms_64, ms_e2e = vals.tolist()
     if rank == 0:
-        steps_total = K * world
+        units = K * world * wl.units
         line = {
-            "metric": METRIC, "value": steps_total / (ms_mx / 1e3), "unit": "load steps/s", "n_gpus": world,
-            "steps": K, "warmup": W, "ms_per_step": ms_mx / K, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
-            "config": dict(WORKLOAD, parallelism=f"replicas x{world}", global_batch=world, seq_len=None,
-                           timed_load_steps=f"{W}..{W + K - 1} of {N_STEPS_TOTAL} (after {W} warm-up steps)",
+            "metric": wl.metric, "value": units / (ms_mx / 1e3), "unit": wl.metric.split(" (")[0],
+            "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_mx / K, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
+            "config": dict(wl.config, parallelism=f"replicas x{world}", global_batch=world * wl.units, seq_len=None,
+                           timed_load_steps=f"{W}..{W + K - 1} of {wl.n_steps} (after {W} warm-up steps)",
                            l2="a 256 MB buffer is written before every timed load step (L2 flush, inside the "
                               "timed region)",
                            small=bool(args.small)),
-            "plain_fp64": {"value": steps_total / (ms_64 / 1e3), "ms_per_step": ms_64 / K},
+            "plain_fp64": {"value": units / (ms_64 / 1e3), "ms_per_step": ms_64 / K},
             "mixed_over_fp64": ms_64 / ms_mx,
-            "rel_err_vs_fp64": {"displacement": rel_disp, "cauchy_stress": rel_sig, "footing_force": rel_force,
-                                "grad_E": rel_grad, "norm": "max-abs difference / max-abs FP64 value"},
-            "e2e": {"value": steps_total / (ms_e2e / 1e3), "unit": "load steps/s", "h2d_bytes_per_step": h2d,
+            "rel_err_vs_fp64": errs,
+            "e2e": {"value": units / (ms_e2e / 1e3), "unit": wl.metric.split(" (")[0], "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(launches),
-            "newton": {"mixed_iters": newton_stats(s_mx.engine), "fp64_iters": newton_stats(s_64.engine)},
+            "newton": newton,
             "roofline": roof,
             "clocks": clocks,
         }
-        line["cpu_baseline"] = cpu_baseline(fk, line)
+        line["cpu_baseline"] = cpu_baseline(wl, line)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()
@@ -259,24 +338,31 @@ def newton_stats(engine):
             "mean_krylov_per_newton": float(np.mean(kry)) if kry else None}
 
 
-def roofline_pass(s, adj, k, fk, dev):
+def roofline_pass(adj, k, wl):
     """Time the dominant kernel family with CUDA events inside one more step."""
     import json as _json
     from geowarp_b200 import profiling
-    peaks = _json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
-        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peaks = _json.load(open(path)) if os.path.exists(path) else {"hbm_gbs": 6650.0}
     with profiling.kernel_timer() as kt:
-        adj.forward_step(k, N_STEPS_TOTAL, keep=False)
-        adj.seed_displacement_misfit()
+        adj.forward_step(k, wl.n_steps, keep=False)
+        wl.seed(adj, k)
         adj.backward_step()
     return profiling.roofline_summary(kt, peaks, peak_kind="measured" if "when" in peaks else "fallback")
 
 
-def cpu_baseline(fk, gpu_line):
-    """Oracle (CPU restatement) timing on a bounded sample, run on rank 0."""
+def cpu_baseline(wl, gpu_line):
+    """Oracle (CPU restatement) timing on a bounded sample, run on rank 0: one
+    load step of the 64x32-cell footing variant, scaled to the workload's
+    particle count."""
     from oracle.bench_sample import oracle_load_step_sample
     sec, its, sample = oracle_load_step_sample()
-    return {"value": 1.0 / sec, "unit": "load steps/s", "cores": 1, "kind": "port",
+    scale = 1.0
+    if isinstance(wl, BatchedWorkload):
+        # per-particle work dominates the oracle step: scale by particles
+        scale = wl.config["particles"] / 131072.0
+        sample += f"; scaled to the batch by x{scale:.2f} (particles)"
+    return {"value": wl.units / (sec * scale), "unit": gpu_line["unit"], "cores": 1, "kind": "port",
             "sample": sample + " (forward load step; the CPU path has no adjoint)"}
 
 
@@ -295,26 +381,31 @@ def run_reference(args):
     for k in range(max(1, min(args.steps, 2))):
         sec, its, sample = oracle_load_step_sample(step=k)
         times.append(sec)
-    v = 1.0 / float(np.mean(times))
+    wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
+    scale = wl.config["particles"] / 131072.0 if isinstance(wl, BatchedWorkload) else 1.0
+    if scale != 1.0:
+        sample += f"; scaled to the batch by x{scale:.2f} (particles)"
+    v = wl.units / (float(np.mean(times)) * scale)
+    unit = wl.metric.split(" (")[0]
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "load steps/s", "n_gpus": world,
+        "impl": "reference", "metric": wl.metric, "value": v, "unit": unit, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "dtype": "f64", "data": "synthetic", "config": dict(WORKLOAD, parallelism="host cores x1"),
-        "cpu_baseline": {"value": v, "unit": "load steps/s", "cores": 1, "kind": "port",
+        "dtype": "f64", "data": "synthetic", "config": dict(wl.config, parallelism="host cores x1"),
+        "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port",
                          "sample": sample + " (forward load step; the CPU path has no adjoint)"},
-        "e2e": {"value": v, "unit": "load steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
 def run_ncu_target(args):
     import torch
-    from geowarp_b200 import problems
-    from geowarp_b200.adjoint import LoadStepAdjoint
-    s = problems.strip_footing_2d(precision="mixed", **footing_kwargs(args.small))
-    adj = LoadStepAdjoint(s)
+    wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
+    if hasattr(wl, "prepare"):
+        wl.prepare(args.warmup + args.steps, torch.device("cuda"))
+    s, adj = wl.make("mixed", torch.device("cuda"))
     for k in range(args.warmup + args.steps):
-        adj.forward_step(k, N_STEPS_TOTAL, keep=False)
-        adj.seed_displacement_misfit()
+        adj.forward_step(k, wl.n_steps, keep=False)
+        wl.seed(adj, k)
         adj.backward_step()
     torch.cuda.synchronize()
     print("ncu target done", len(s.engine.log), "Newton iterations")

@@ -43,7 +43,10 @@ class DofStruct:
 
 class quasi_static_solver_2d:
     def __init__(self, background_grid_dict, particles_dict, iteration_dict, material_dict, load_dict,
-                 precision="fp64", device=None, precond="mg"):
+                 precision="fp64", device=None, precond="mg", x_particles=None):
+        """x_particles (extension): particle positions [n_particles, 2] to use
+        instead of the regular seeding of the start/end box (e.g. several
+        separate blocks in one grid)."""
         g = background_grid_dict
         self.n_grid_x = g["n_grid_x"]
         self.n_grid_y = g["n_grid_y"]
@@ -87,8 +90,11 @@ class quasi_static_solver_2d:
         self.point_load_value_y = load_dict.get("point_load_value_y", 0.0)
         self.load_dict = dict(load_dict)
 
-        x = init_particles_rectangle_2d(self.start_x, self.start_y, self.end_x, self.end_y, self.dx, self.n_grid_x,
-                                        self.n_grid_y, self.PPD, self.n_particles)
+        if x_particles is None:
+            x = init_particles_rectangle_2d(self.start_x, self.start_y, self.end_x, self.end_y, self.dx, self.n_grid_x,
+                                            self.n_grid_y, self.PPD, self.n_particles)
+        else:
+            x = np.asarray(x_particles, dtype=np.float64).reshape(self.n_particles, 2)
         self.engine = Engine("solid2d", (self.n_grid_x, self.n_grid_y), (self.dx, self.dx), (self.dx, self.dx),
                              (self.domain_min_x, self.domain_min_y), (self.domain_max_x, self.domain_max_y), x,
                              device=device, precision=precision, precond=precond)
