@@ -40,11 +40,12 @@ inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
 // algorithmic bytes the host attributed to each launch.
 enum ProfClass {
     PC_ASSEMBLE = 0, PC_SPMV, PC_DOTS, PC_UPDATE, PC_NEXT, PC_G2P, PC_ADJ_G2P, PC_ADJ_RES,
-    PC_MG_JACOBI, PC_MG_RESID, PC_MG_TRANSFER, PC_MG_SETUP, PC_COUNT
+    PC_MG_JACOBI, PC_MG_RESID, PC_MG_TRANSFER, PC_MG_SETUP, PC_MG_JACOBI_COARSE, PC_COUNT
 };
 const char *kProfNames[PC_COUNT] = {"k_assemble", "k_gm_spmv", "k_gm_dots", "k_gm_update", "k_gm_next", "k_g2p",
-                                    "k_adjoint_g2p", "k_adjoint_residual", "k_mg_jacobi", "k_mg_residual",
-                                    "k_mg_restrict/prolong", "mg_setup"};
+                                    "k_adjoint_g2p", "k_adjoint_residual", "k_mg_jacobi (finest level)",
+                                    "k_mg_residual", "k_mg_restrict/prolong", "mg_setup",
+                                    "k_mg_jacobi (coarse levels)"};
 struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
 bool g_prof_on = false;
 ProfRec *g_prof = nullptr;
@@ -862,7 +863,8 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
     const int g = zero ? red_grid_elems(v.A.n_rows) : red_grid_rows(v.A.n_rows);
     // algorithmic bytes: b, x_out, Minv; with a previous iterate also x_in and the matrix
     const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
-    ProfScope ps(PC_MG_JACOBI, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
+    ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
+                 2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
     if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), kThreads, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
     else k_mg_jacobi<NF, double><<<gw_count_launch(g), kThreads, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
 }

@@ -361,10 +361,10 @@ int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *mat, const g
 
 /* ------------------------------------------------------------ kernel timing
  * Optional CUDA-event timing of the engine's main kernels (off by default):
- * classes 0..11 = k_assemble, k_gm_spmv, k_gm_dots, k_gm_update, k_gm_next,
- * k_g2p, k_adjoint_g2p, k_adjoint_residual, k_mg_jacobi, k_mg_residual,
- * k_mg_restrict/prolong, mg_setup (the whole hierarchy build, host reads
- * included).  gw_profile_read synchronises and
+ * classes 0..12 = k_assemble, k_gm_spmv, k_gm_dots, k_gm_update, k_gm_next,
+ * k_g2p, k_adjoint_g2p, k_adjoint_residual, k_mg_jacobi (finest level),
+ * k_mg_residual, k_mg_restrict/prolong, mg_setup (the numeric hierarchy
+ * build), k_mg_jacobi (coarse levels).  gw_profile_read synchronises and
  * returns the total time, launch count and algorithmic bytes of a class. */
 int gw_profile_enable(int32_t on);
 /* Number of timing classes (k_assemble ... mg_setup) gw_profile_read accepts. */
