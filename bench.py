@@ -185,15 +185,11 @@ class BatchedWorkload:
 # ------------------------------------------------------------------ GPU arm
 def run_geowarp(args):
     import torch
-    import torch.distributed as dist
     from geowarp_b200 import _lib as L
+    from geowarp_b200.replicas import Replicas, aggregate_rate
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+    rep = Replicas("nccl")  # one independent replica per GPU (no data-path collective)
+    world, rank = rep.world, rep.rank
     dev = torch.device("cuda", torch.cuda.current_device())
     wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
     W, K = args.warmup, args.steps
@@ -205,8 +201,7 @@ def run_geowarp(args):
 
     def sync():
         torch.cuda.synchronize(dev)
-        if world > 1:
-            dist.barrier()
+        rep.barrier()
 
     def one_step(adj, k):
         # forward load step (checkpointed), then its adjoint seeded with the
@@ -294,14 +289,12 @@ def run_geowarp(args):
     # ---- dominant kernel, instrumented pass on one more step (not part of value)
     roof = roofline_pass(adj_mx, W + K, wl)
 
-    vals = torch.tensor([ms_mx, ms_64, ms_e2e], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-    ms_mx, ms_64, ms_e2e = vals.tolist()
+    ms_mx, ms_64, ms_e2e = rep.max_over_ranks([ms_mx, ms_64, ms_e2e], device=dev)
     if rank == 0:
         units = K * world * wl.units
         line = {
-            "metric": wl.metric, "value": units / (ms_mx / 1e3), "unit": wl.metric.split(" (")[0],
+            "metric": wl.metric, "value": aggregate_rate([K * wl.units] * world, ms_mx),
+            "unit": wl.metric.split(" (")[0],
             "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": ms_mx / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
             "config": dict(wl.config, parallelism=f"replicas x{world}", global_batch=world * wl.units, seq_len=None,
@@ -321,9 +314,7 @@ def run_geowarp(args):
         }
         line["cpu_baseline"] = cpu_baseline(wl, line)
         print(json.dumps(line))
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    rep.close()
 
 
 def newton_stats(engine):
