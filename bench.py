@@ -12,6 +12,11 @@ the same steps for the error check and is reported beside it.  With N GPUs
 the job runs N independent replicas (one per rank; there is no data-path
 collective) and `value` is the aggregate over ranks.
 
+--workload batched runs 64 inverse-analysis blocks packed into one engine;
+--workload consolidation runs the 1 x 200-cell coupled u-p column (forward
+load steps with their own time increments; the adjoint covers the 2D solid
+solver).
+
 --impl reference times the CPU restatement of the reference's algorithm (the
 reference itself runs only on NVIDIA Warp, not installable here) on a bounded
 sample of the same workload.
@@ -46,8 +51,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geowarp", choices=["geowarp", "reference"])
     ap.add_argument("--small", action="store_true", help="64x32-cell variant for quick checks")
-    ap.add_argument("--workload", default="footing", choices=["footing", "batched"],
-                    help="footing: the strip footing (default); batched: 64 inverse-analysis blocks in one engine")
+    ap.add_argument("--workload", default="footing", choices=["footing", "batched", "consolidation"],
+                    help="footing: the strip footing (default); batched: 64 inverse-analysis blocks in one engine; "
+                         "consolidation: the 1 x 200-cell u-p column (forward load steps)")
     ap.add_argument("--instances", type=int, default=64, help="blocks of the batched workload")
     ap.add_argument("--profile", action="store_true", help="also time the dominant kernel (instrumented pass)")
     ap.add_argument("--ncu", action="store_true",
@@ -109,7 +115,18 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------------ workloads
-class FootingWorkload:
+class Workload:
+    """A timed unit: step(adj, k) runs load step k forward (checkpointed) and
+    then its adjoint seeded by the workload's misfit."""
+    adjoint = True
+
+    def step(self, adj, k):
+        adj.forward_step(k, self.n_steps, keep=False)
+        self.seed(adj, k)
+        adj.backward_step()
+
+
+class FootingWorkload(Workload):
     """The strip footing: one instance per load step."""
 
     def __init__(self, args):
@@ -132,7 +149,7 @@ class FootingWorkload:
         return {"footing_force": abs(s_mx.footing_force - s_64.footing_force) / abs(s_64.footing_force)}
 
 
-class BatchedWorkload:
+class BatchedWorkload(Workload):
     """Batched inverse analysis: n self-weight blocks (cell counts seeded
     uniformly in 32x32..128x64, per-particle log E a Gaussian random field)
     in one engine; each load step is forward + adjoint of the summed
@@ -182,6 +199,62 @@ class BatchedWorkload:
         return {}
 
 
+class ConsolidationStepper:
+    """Forward load steps of the consolidation column, each with its own time
+    increment."""
+
+    def __init__(self, solver, dts):
+        self.solver, self.dts = solver, dts
+
+    def forward_step(self, k, n_steps, keep=False):
+        self.solver.dt = float(self.dts[k])
+        self.solver.advance_one_step(k, n_steps)
+
+
+class ConsolidationWorkload(Workload):
+    """Coupled u-p 1D consolidation: 1 x 200 cells of 0.05 m, 2 x 2 particles
+    per cell, linear elastic skeleton; forward load steps only (the
+    hand-written adjoint covers the 2D solid solver)."""
+    adjoint = False
+
+    def __init__(self, args):
+        from geowarp_b200 import problems
+        self.dicts = problems.consolidation_column_dicts()
+        self.dts = self.dicts[6]
+        self.units = 1
+        self.n_steps = len(self.dts)
+        self.config = dict(workload="2D coupled u-p 1D consolidation column",
+                           cells="1x200 cells (6x202 grid), dx=0.05 m", particles=800, ppc="2x2",
+                           material="linear elastic skeleton E=1e7 Pa nu=0.3; permeability 1e-10 m2, fluid viscosity "
+                                    "1e-3 Pa.s (mobility 1e-7), porosity 0.4",
+                           load="10 kPa surface traction, drained top, undrained fixed base, roller sides",
+                           time_steps="200 geometrically growing increments from mesh Fourier number cv dt/dx^2 = 4 "
+                                      "to a Terzaghi time factor of 2",
+                           solver="flexible GMRES(30) + multigrid V-cycle with Schur-diagonal pressure smoother")
+        self.metric = "load steps/s (forward; u-p), mixed vs plain FP64 on same B200"
+
+    def make(self, precision, dev):
+        from geowarp_b200 import problems
+        s, dts, cv, H = problems.consolidation_column_2d(precision=precision, device=dev)
+        return s, ConsolidationStepper(s, dts)
+
+    def step(self, adj, k):
+        adj.forward_step(k, self.n_steps)
+
+    def errors(self, s_mx, s_64):
+        q = 1e4
+        return {"pore_pressure_over_load": float((s_mx.particle_pressure_array - s_64.particle_pressure_array)
+                                                 .abs().max() / q)}
+
+
+def make_workload(args):
+    if args.workload == "batched":
+        return BatchedWorkload(args)
+    if args.workload == "consolidation":
+        return ConsolidationWorkload(args)
+    return FootingWorkload(args)
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_geowarp(args):
     import torch
@@ -191,8 +264,11 @@ def run_geowarp(args):
     rep = Replicas("nccl")  # one independent replica per GPU (no data-path collective)
     world, rank = rep.world, rep.rank
     dev = torch.device("cuda", torch.cuda.current_device())
-    wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
+    wl = make_workload(args)
     W, K = args.warmup, args.steps
+    if W + K + 1 > wl.n_steps:
+        raise SystemExit(f"--warmup + --steps + 1 (the instrumented step) must not exceed the workload's "
+                         f"{wl.n_steps} load steps")
     if hasattr(wl, "prepare"):
         wl.prepare(W + K + 1, dev)
     lib = L.load()
@@ -204,11 +280,9 @@ def run_geowarp(args):
         rep.barrier()
 
     def one_step(adj, k):
-        # forward load step (checkpointed), then its adjoint seeded with the
-        # displacement misfit
-        adj.forward_step(k, wl.n_steps, keep=False)
-        wl.seed(adj, k)
-        adj.backward_step()
+        # forward load step (checkpointed), then (where the workload has one)
+        # its adjoint seeded with the displacement misfit
+        wl.step(adj, k)
 
     # ---- mixed precision, resident (value)
     s_mx, adj_mx = wl.make("mixed", dev)
@@ -247,7 +321,9 @@ def run_geowarp(args):
             "cauchy_stress": float((s_mx.particle_Cauchy_stress_array - s_64.particle_Cauchy_stress_array).abs().max()
                                    / s_64.particle_Cauchy_stress_array.abs().max())}
     errs.update(wl.errors(s_mx, s_64))
-    errs["grad_E"] = float((adj_mx.grad_E - adj_64.grad_E).abs().max() / adj_64.grad_E.abs().max().clamp_min(1e-300))
+    if wl.adjoint:
+        errs["grad_E"] = float((adj_mx.grad_E - adj_64.grad_E).abs().max()
+                               / adj_64.grad_E.abs().max().clamp_min(1e-300))
     errs["norm"] = "max-abs difference / max-abs FP64 value"
     newton = {"mixed_iters": newton_stats(s_mx.engine), "fp64_iters": newton_stats(s_64.engine)}
     del s_64, adj_64
@@ -265,6 +341,9 @@ def run_geowarp(args):
     for name in state:
         host[name].copy_(getattr(e, name))
     sigma_host = torch.empty_like(e.sigma, device="cpu").pin_memory()
+    # the step's result: the gradient (fwd+adjoint workloads) or the particle
+    # pore pressure (forward u-p workloads)
+    out_dev = (lambda: adj_e2e.grad_E) if wl.adjoint else (lambda: e.pressure)
     grad_host = torch.empty(e.N, dtype=torch.float64).pin_memory()
     sync()
     h2d = sum(t.numel() * t.element_size() for t in host.values())
@@ -278,7 +357,7 @@ def run_geowarp(args):
         for name in state:
             host[name].copy_(getattr(e, name), non_blocking=True)
         sigma_host.copy_(e.sigma, non_blocking=True)
-        grad_host.copy_(adj_e2e.grad_E, non_blocking=True)
+        grad_host.copy_(out_dev(), non_blocking=True)
         torch.cuda.current_stream(dev).synchronize()
     ev1.record()
     sync()
@@ -336,9 +415,7 @@ def roofline_pass(adj, k, wl):
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     peaks = _json.load(open(path)) if os.path.exists(path) else {"hbm_gbs": 6650.0}
     with profiling.kernel_timer() as kt:
-        adj.forward_step(k, wl.n_steps, keep=False)
-        wl.seed(adj, k)
-        adj.backward_step()
+        wl.step(adj, k)
     return profiling.roofline_summary(kt, peaks, peak_kind="measured" if "when" in peaks else "fallback")
 
 
@@ -346,6 +423,10 @@ def cpu_baseline(wl, gpu_line):
     """Oracle (CPU restatement) timing on a bounded sample, run on rank 0: one
     load step of the 64x32-cell footing variant, scaled to the workload's
     particle count."""
+    if isinstance(wl, ConsolidationWorkload):
+        from oracle.bench_sample import oracle_consolidation_sample
+        sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts)
+        return {"value": 1.0 / sec, "unit": gpu_line["unit"], "cores": 1, "kind": "port", "sample": sample}
     from oracle.bench_sample import oracle_load_step_sample
     sec, its, sample = oracle_load_step_sample()
     scale = 1.0
@@ -367,37 +448,41 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from oracle.bench_sample import oracle_load_step_sample
-    times = []
-    for k in range(max(1, min(args.steps, 2))):
-        sec, its, sample = oracle_load_step_sample(step=k)
-        times.append(sec)
-    wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
-    scale = wl.config["particles"] / 131072.0 if isinstance(wl, BatchedWorkload) else 1.0
-    if scale != 1.0:
-        sample += f"; scaled to the batch by x{scale:.2f} (particles)"
-    v = wl.units / (float(np.mean(times)) * scale)
+    wl = make_workload(args)
+    if isinstance(wl, ConsolidationWorkload):
+        from oracle.bench_sample import oracle_consolidation_sample
+        sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts, max_steps=max(args.steps, 3),
+                                                     budget_s=60.0)
+        v = 1.0 / sec
+    else:
+        from oracle.bench_sample import oracle_load_step_sample
+        times = []
+        for k in range(max(1, min(args.steps, 2))):
+            sec, its, sample = oracle_load_step_sample(step=k)
+            times.append(sec)
+        scale = wl.config["particles"] / 131072.0 if isinstance(wl, BatchedWorkload) else 1.0
+        if scale != 1.0:
+            sample += f"; scaled to the batch by x{scale:.2f} (particles)"
+        sample += " (forward load step; the CPU path has no adjoint)"
+        v = wl.units / (float(np.mean(times)) * scale)
     unit = wl.metric.split(" (")[0]
     print(json.dumps({
         "impl": "reference", "metric": wl.metric, "value": v, "unit": unit, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
         "dtype": "f64", "data": "synthetic", "config": dict(wl.config, parallelism="host cores x1"),
-        "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port",
-                         "sample": sample + " (forward load step; the CPU path has no adjoint)"},
+        "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
 def run_ncu_target(args):
     import torch
-    wl = BatchedWorkload(args) if args.workload == "batched" else FootingWorkload(args)
+    wl = make_workload(args)
     if hasattr(wl, "prepare"):
         wl.prepare(args.warmup + args.steps, torch.device("cuda"))
     s, adj = wl.make("mixed", torch.device("cuda"))
     for k in range(args.warmup + args.steps):
-        adj.forward_step(k, wl.n_steps, keep=False)
-        wl.seed(adj, k)
-        adj.backward_step()
+        wl.step(adj, k)
     torch.cuda.synchronize()
     print("ncu target done", len(s.engine.log), "Newton iterations")
 

@@ -818,7 +818,7 @@ int mg_numeric(MgHier &h, cudaStream_t s) {
     {
         const MgLevel &l0 = h.lv[0];
         PtrsA a0 = make_ptrs(l0.A);
-        k_precond_setup<NF, VT><<<gw_count_launch(nblk(l0.A.n_rows, kThreads)), kThreads, 0, s>>>(a0, D, 1, l0.Minv);
+        k_mg_smoother_setup<NF, VT><<<gw_count_launch(nblk(l0.A.n_rows, kThreads)), kThreads, 0, s>>>(a0, D, l0.Minv);
         k_mg_fixed_mask<NF, VT><<<gw_count_launch(nblk(l0.A.n_rows, kThreads)), kThreads, 0, s>>>(a0, l0.fixed);
         GW_LAUNCHED();
     }
@@ -836,7 +836,7 @@ int mg_numeric(MgHier &h, cudaStream_t s) {
         GW_LAUNCHED();
         const int nrc = c.A.n_rows;
         k_mg_fix_empty_rows<NF><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca);
-        k_precond_setup<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, D, 1, c.Minv);
+        k_mg_smoother_setup<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, D, c.Minv);
         k_mg_fixed_mask<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, c.fixed);
         GW_LAUNCHED();
     }

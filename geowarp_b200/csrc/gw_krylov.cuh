@@ -140,32 +140,14 @@ __global__ void k_spmv_t(PtrsA A, const double *__restrict__ x, double *__restri
 }
 
 // ---------------------------------------------------------------- preconditioner
-// Minv: per row an NF x NF block.  mode 0: inverse of the scalar diagonal
-// (zero diagonal -> 1, as a Jacobi guard), mode 1: inverse of the diagonal block.
-template <int NF, typename VT>
-__global__ void k_precond_setup(PtrsA A, int D, int mode, double *__restrict__ Minv) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= A.n_rows) return;
-    const int node = A.row2node[r];
-    const int off[3] = {0, 0, 0};
-    const int bit = D == 2 ? offset_bit<2>(off) : offset_bit<3>(off);
-    const int slot = stencil_slot(A.stencil, A.mw, node, bit);
-    double *out = Minv + (size_t)r * NF * NF;
-    if (slot < 0) {  // no diagonal block: identity preconditioner on this row
-        for (int i = 0; i < NF; ++i)
-            for (int j = 0; j < NF; ++j) out[i * NF + j] = (i == j) ? 1.0 : 0.0;
-        return;
-    }
-    const VT *blk = (const VT *)A.vals + ((size_t)A.row_ptr[r] + slot) * NF * NF;
+// Inverse of one NF x NF block by Gauss-Jordan with partial pivoting, into
+// out (row-major).  A singular block falls back to the inverse of its
+// diagonal (zero diagonal entries -> 1).
+template <int NF>
+__device__ __forceinline__ void invert_block(const double Min[NF][NF], double *__restrict__ out) {
     double M[NF][NF], I[NF][NF];
     for (int i = 0; i < NF; ++i)
-        for (int j = 0; j < NF; ++j) { M[i][j] = (double)blk[i * NF + j]; I[i][j] = (i == j) ? 1.0 : 0.0; }
-    if (mode == 0) {
-        for (int i = 0; i < NF; ++i)
-            for (int j = 0; j < NF; ++j) out[i * NF + j] = (i == j) ? (M[i][i] != 0.0 ? 1.0 / M[i][i] : 1.0) : 0.0;
-        return;
-    }
-    // Gauss-Jordan with partial pivoting; singular blocks fall back to the diagonal
+        for (int j = 0; j < NF; ++j) { M[i][j] = Min[i][j]; I[i][j] = (i == j) ? 1.0 : 0.0; }
     bool ok = true;
     for (int cidx = 0; cidx < NF; ++cidx) {
         int piv = cidx;
@@ -187,8 +169,36 @@ __global__ void k_precond_setup(PtrsA A, int D, int mode, double *__restrict__ M
     for (int i = 0; i < NF; ++i)
         for (int j = 0; j < NF; ++j) {
             if (ok) out[i * NF + j] = I[i][j];
-            else out[i * NF + j] = (i == j) ? ((double)blk[i * NF + i] != 0.0 ? 1.0 / (double)blk[i * NF + i] : 1.0) : 0.0;
+            else out[i * NF + j] = (i == j) ? (Min[i][i] != 0.0 ? 1.0 / Min[i][i] : 1.0) : 0.0;
         }
+}
+
+// Minv: per row an NF x NF block.  mode 0: inverse of the scalar diagonal
+// (zero diagonal -> 1, as a Jacobi guard), mode 1: inverse of the diagonal block.
+template <int NF, typename VT>
+__global__ void k_precond_setup(PtrsA A, int D, int mode, double *__restrict__ Minv) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n_rows) return;
+    const int node = A.row2node[r];
+    const int off[3] = {0, 0, 0};
+    const int bit = D == 2 ? offset_bit<2>(off) : offset_bit<3>(off);
+    const int slot = stencil_slot(A.stencil, A.mw, node, bit);
+    double *out = Minv + (size_t)r * NF * NF;
+    if (slot < 0) {  // no diagonal block: identity preconditioner on this row
+        for (int i = 0; i < NF; ++i)
+            for (int j = 0; j < NF; ++j) out[i * NF + j] = (i == j) ? 1.0 : 0.0;
+        return;
+    }
+    const VT *blk = (const VT *)A.vals + ((size_t)A.row_ptr[r] + slot) * NF * NF;
+    double M[NF][NF];
+    for (int i = 0; i < NF; ++i)
+        for (int j = 0; j < NF; ++j) M[i][j] = (double)blk[i * NF + j];
+    if (mode == 0) {
+        for (int i = 0; i < NF; ++i)
+            for (int j = 0; j < NF; ++j) out[i * NF + j] = (i == j) ? (M[i][i] != 0.0 ? 1.0 / M[i][i] : 1.0) : 0.0;
+        return;
+    }
+    invert_block<NF>(M, out);
 }
 
 template <int NF>

@@ -15,6 +15,17 @@
 //   smoother: damped node-block Jacobi; coarsest level (at most 40 unknowns):
 //     explicit dense inverse.
 //
+// Coupled u-p systems (D displacement fields and one pressure field per node)
+// are saddle points [[K, B], [B^T, -C]] whose u-p coupling lives off the node
+// diagonal (the node's own B entries vanish) and whose pressure block C =
+// dt k Laplacian is tiny at small time steps.  Plain node-block Jacobi then
+// updates the pressure by r_p / C, which diverges once B^2 / (C K) > 1 (mesh
+// Fourier number cv dt / dx^2 below about one).  The smoother therefore
+// inverts node blocks whose pressure diagonal is replaced by that of the
+// Schur complement with a diagonal K:
+//   S_ii = -C_ii - sum_{j != i} sum_g B_i(j,g) B^T(j,g)_i / K(j,g; j,g),
+// the diagonal-approximation Schur smoother of SIMPLE-type block methods.
+//
 // Fixed (Dirichlet) DOFs are recognised from the Jacobian: their rows are
 // identity rows (the assembly writes 1 on the diagonal and nothing else).
 #pragma once
@@ -238,6 +249,62 @@ __global__ void k_mg_fix_empty_rows(PtrsA A) {
                 if (vals[(size_t)j * NF * NF + f * NF + g] != 0.0) { empty = false; break; }
         if (empty) vals[(size_t)self * NF * NF + f * NF + f] = 1.0;
     }
+}
+
+// ---------------------------------------------------------------- smoother blocks
+// Minv of one level: inverse of each node's diagonal block; on u-p systems
+// (NF == D + 1) the pressure diagonal first takes the off-node Schur term.
+// A row's blocks are stored in stencil-bit order, the bit of offset o being
+// sum_k (o_k + 2) 5^k, so the transposed block (j, i) of block (i, j) sits at
+// bit (5^D - 1) - bit in row j.
+template <int NF, typename VT>
+__global__ void k_mg_smoother_setup(PtrsA A, int D, double *__restrict__ Minv) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= A.n_rows) return;
+    const int node = A.row2node[r];
+    const int top = D == 2 ? 24 : 124;  // 5^D - 1
+    const int center = top / 2;
+    const int slot = stencil_slot(A.stencil, A.mw, node, center);
+    double *out = Minv + (size_t)r * NF * NF;
+    if (slot < 0) {
+        for (int i = 0; i < NF; ++i)
+            for (int j = 0; j < NF; ++j) out[i * NF + j] = (i == j) ? 1.0 : 0.0;
+        return;
+    }
+    const VT *vals = (const VT *)A.vals;
+    const VT *blk = vals + ((size_t)A.row_ptr[r] + slot) * NF * NF;
+    double M[NF][NF];
+    for (int i = 0; i < NF; ++i)
+        for (int j = 0; j < NF; ++j) M[i][j] = (double)blk[i * NF + j];
+    if (NF == D + 1) {
+        constexpr int P = NF - 1;
+        double corr = 0.0;
+        int s = 0;
+        for (int w = 0; w < A.mw; ++w) {
+            uint32_t m = A.stencil[(size_t)node * A.mw + w];
+            while (m) {
+                const int bit = w * 32 + __ffs(m) - 1;
+                m &= m - 1u;
+                const int k = A.row_ptr[r] + s++;
+                if (bit == center) continue;
+                const int col = A.cols[k];
+                const int nj = A.row2node[col];
+                const int tj = stencil_slot(A.stencil, A.mw, nj, top - bit);
+                const int dj = stencil_slot(A.stencil, A.mw, nj, center);
+                if (tj < 0 || dj < 0) continue;
+                const VT *b_ij = vals + (size_t)k * NF * NF;
+                const VT *b_ji = vals + ((size_t)A.row_ptr[col] + tj) * NF * NF;
+                const VT *b_jj = vals + ((size_t)A.row_ptr[col] + dj) * NF * NF;
+#pragma unroll
+                for (int g = 0; g < P; ++g) {
+                    const double kjj = (double)b_jj[g * NF + g];
+                    if (kjj != 0.0) corr += (double)b_ij[P * NF + g] * (double)b_ji[g * NF + P] / kjj;
+                }
+            }
+        }
+        M[P][P] -= corr;
+    }
+    invert_block<NF>(M, out);
 }
 
 // ---------------------------------------------------------------- cycle kernels

@@ -114,3 +114,129 @@ def strip_footing_2d(precision="fp64", device=None, K0=None, **kw):
             K0 = 1.0 - np.sin(np.radians(mat["friction_angle"]))
         geostatic_stress(s, grid["end_y"], parts["p_rho"], load["gravity_mag"], K0)
     return s
+
+
+# ---------------------------------------------------------------- bar compaction (self-weight)
+def bar_compaction_2d(precision="fp64", device=None, width_cells=4, height_cells=40, dx=0.25, PPD=2, E=1e6, nu=0.3,
+                      rho=80.0, gravity=9.81, material="Neo-Hookean", n_iter=20, tol=1e-6, precond="mg"):
+    """A bar width_cells x height_cells cells under self-weight ramped over the
+    load steps (problems/bar_compaction/bar_compaction_cpGIMP.py): rollers on
+    both side walls, fixed base, two empty cells around it."""
+    pad = 2
+    n_grid_x, n_grid_y = width_cells + 2 * pad, height_cells + 2 * pad
+    sx, sy = pad * dx, pad * dx
+    ex, ey = sx + width_cells * dx, sy + height_cells * dx
+    grid = dict(n_grid_x=n_grid_x, n_grid_y=n_grid_y, max_x=n_grid_x * dx, dx=dx, start_x=sx, end_x=ex,
+                start_y=sy, end_y=ey, domain_min_x=sx, domain_max_x=ex, domain_min_y=sy, domain_max_y=ey)
+    parts = dict(n_particles=width_cells * height_cells * PPD * PPD, PPD=PPD, p_vol=(dx / PPD) ** 2, p_rho=rho)
+    it = dict(n_iter=n_iter, tol=tol, solver_name="warp")
+    mat = dict(youngs_modulus=E, poisson_ratio=nu, material_name=material)
+    load = dict(gravity_mag=gravity, traction_value_x=0.0, traction_value_y=0.0, point_load_value_x=0.0,
+                point_load_value_y=0.0)
+    s = quasi_static_solver_2d(grid, parts, it, mat, load, precision=precision, device=device, precond=precond)
+    nx1 = n_grid_x + 1
+    nn = nx1 * (n_grid_y + 1)
+    ix = np.tile(np.arange(nx1), n_grid_y + 1)
+    iy = np.repeat(np.arange(n_grid_y + 1), nx1)
+    b = np.zeros(2 * nn, dtype=bool)
+    b[((ix <= pad) | (ix >= pad + width_cells)).nonzero()[0]] = True
+    b[(iy <= pad).nonzero()[0]] = True
+    b[(iy <= pad).nonzero()[0] + nn] = True
+    s.dofStruct.boundary_flag_array[:] = torch.as_tensor(b, device=s.x_particles.device)
+    return s
+
+
+# ---------------------------------------------------------------- 1D consolidation (u-p)
+def terzaghi_pressure(z_from_drained, t, H, cv, q, terms=200):
+    """Terzaghi's excess pore pressure in a layer of height H drained on one
+    face and undrained on the other, under a sudden surface load q:
+    p = q sum_m (2/M) sin(M z/H) exp(-M^2 T),  M = pi (2m+1)/2,  T = cv t / H^2."""
+    z = np.asarray(z_from_drained, dtype=np.float64)
+    T = cv * t / H ** 2
+    p = np.zeros_like(z)
+    for m in range(terms):
+        M = np.pi * (2 * m + 1) / 2
+        p += 2.0 / M * np.sin(M * z / H) * np.exp(-M * M * T)
+    return q * p
+
+
+def consolidation_dts(n_steps, dt_first, t_end):
+    """n_steps geometrically growing time increments dt_first r^k summing to t_end."""
+    if dt_first * n_steps >= t_end:
+        raise ValueError("dt_first * n_steps must stay below t_end")
+    lo, hi = 1.0, 2.0
+    while dt_first * (hi ** n_steps - 1) / (hi - 1) < t_end:
+        hi *= 2.0
+    for _ in range(200):
+        r = 0.5 * (lo + hi)
+        if dt_first * (r ** n_steps - 1) / (r - 1) < t_end:
+            lo = r
+        else:
+            hi = r
+    dts = dt_first * (0.5 * (lo + hi)) ** np.arange(n_steps)
+    return dts * (t_end / dts.sum())
+
+
+def consolidation_column_dicts(n_cells=200, dx=0.05, PPD=2, E=1e7, nu=0.3, permeability=1e-10, viscosity=1e-3,
+                               porosity=0.4, surface_load=1e4, n_steps=200, first_fourier=4.0, T_end=2.0, n_iter=15,
+                               tol=1e-8, material="Linear elasticity"):
+    """Constructor dictionaries of the consolidation column (the layout of
+    problems/consolidation/terzaghi_cpGIMP.py:10-73) plus its time
+    increments: returns (grid, particles, iteration, material, porous, load,
+    dts, cv, H)."""
+    n_grid_x, n_grid_y = 6, n_cells + 2
+    max_y = n_grid_y * dx
+    sx, ex, sy, ey = dx, 2 * dx, 0.0, n_cells * dx
+    grid = dict(n_grid_x=n_grid_x, n_grid_y=n_grid_y, max_x=n_grid_x * dx, dx=dx, max_y=max_y, dy=max_y / n_grid_y,
+                start_x=sx, end_x=ex, start_y=sy, end_y=ey, domain_min_x=sx, domain_max_x=ex, domain_min_y=sy,
+                domain_max_y=max_y)
+    parts = dict(n_particles=n_cells * PPD * PPD, PPD=PPD, p_vol=(dx / PPD) ** 2, p_rho=1.0)
+    H = n_cells * dx
+    mobility = permeability / viscosity
+    M = E * (1 - nu) / ((1 + nu) * (1 - 2 * nu))   # constrained modulus
+    cv = mobility * M
+    dts = consolidation_dts(n_steps, first_fourier * dx * dx / cv, T_end * H * H / cv)
+    it = dict(n_iter=n_iter, tol=tol, solver_name="scipy", dt=float(dts[0]))
+    mat = dict(youngs_modulus=E, poisson_ratio=nu, material_name=material)
+    porous = dict(phi_initial=porosity, mobility_constant=mobility)
+    load = dict(gravity_mag=0.0, traction_value_x=0.0, traction_value_y=-surface_load, point_load_value_x=0.0,
+                point_load_value_y=0.0)
+    return grid, parts, it, mat, porous, load, dts, cv, H
+
+
+def consolidation_boundary_dofs(tid, boundary_flag_array, n_grid_x, n_nodes):
+    """set_boundary_dofs of terzaghi_cpGIMP.py:104-119 on index tensors:
+    x fixed on the side-wall node columns, y fixed on the base row."""
+    ix, iy = tid
+    dof_x = ix + iy * (n_grid_x + 1)
+    boundary_flag_array[dof_x[(ix <= 1) | (ix >= 2)]] = True
+    boundary_flag_array[dof_x[iy <= 0] + n_nodes] = True
+
+
+def consolidation_column_2d(precision="fp64", device=None, precond="mg", krylov_rtol=None, **kw):
+    """One-dimensional consolidation in a column of 1 x n_cells cells
+    (problems/consolidation/terzaghi_cpGIMP.py): linear elastic skeleton,
+    mobility k / mu, drained top with the surface load applied as a traction,
+    undrained fixed base, rollers on the sides.  The n_steps time increments
+    grow geometrically from a mesh Fourier number cv dt / dx^2 of
+    first_fourier up to a Terzaghi time factor T_end = cv t / H^2 in total
+    (keywords of consolidation_column_dicts); returns (solver, dts, cv, H).
+
+    The Newton system is a saddle point (u-p) solved by flexible GMRES with
+    the multigrid V-cycle (Schur-diagonal pressure smoother); node-block
+    Jacobi Krylov stalls on it.  Increments far below one mesh Fourier number
+    make it near-undrained and ill-conditioned for any smoother.  The FP64
+    Krylov tolerance defaults to 1e-10, the reference's BiCGSTAB tolerance:
+    1e-12 lies at the FP64 floor of this system."""
+    from .solvers.quasi_static_coupled_solver_2d import quasi_static_coupled_solver_2d
+    grid, parts, it, mat, porous, load, dts, cv, H = consolidation_column_dicts(**kw)
+    s = quasi_static_coupled_solver_2d(grid, parts, it, mat, porous, load, consolidation_boundary_dofs,
+                                       precision=precision, device=device, precond=precond)
+    if krylov_rtol is not None:
+        s.engine.krylov_rtol = krylov_rtol
+    elif precision == "fp64":
+        s.engine.krylov_rtol = 1e-10
+    top = s.x_particles[:, 1] > grid["end_y"] - grid["dx"] / parts["PPD"]
+    s.particle_pressure_boundary_flag_array[:] = top
+    s.particle_traction_flag_array[:] = top
+    return s, dts, cv, H

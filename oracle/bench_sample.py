@@ -1,6 +1,7 @@
-"""Bounded CPU sample of the strip-footing workload for the benchmark's
-CPU-baseline leg (test infrastructure: the oracle is the checker, timed here
-only as the reported CPU baseline).
+"""Bounded CPU samples of the benchmark workloads (strip footing,
+consolidation column) for the benchmark's CPU-baseline leg (test
+infrastructure: the oracle is the checker, timed here only as the reported
+CPU baseline).
 
 One Newton iteration of load step 0 of the plane-strain Drucker-Prager strip
 footing: residual and complex-step element tangents for every particle
@@ -123,3 +124,54 @@ def oracle_load_step_sample(footing_kwargs=None, full=(256, 128), step=0):
             f"{kw['n_cells_x']}x{kw['n_cells_y']}-cell variant ({o.N} particles, {o.ndof} DOFs), NumPy oracle on "
             f"1 host thread; scaled to the 256x128-cell workload by x{pr:.0f} (particles) and x{dr ** 1.5:.0f} (solve)")
     return est, its, desc
+
+
+def consolidation_oracle(grid, parts, it, mat, porous, load):
+    """The consolidation column in the oracle, from the solver-constructor
+    dictionaries (problems/consolidation/terzaghi_cpGIMP.py:10-73 layout):
+    drained, loaded top particles; the caller passes the boundary callback of
+    terzaghi_cpGIMP.py:104-119 to advance_one_step."""
+    dx = grid["dx"]
+    x = init_particles_rectangle_2d(grid["start_x"], grid["start_y"], grid["end_x"], grid["end_y"], dx,
+                                    grid["n_grid_x"], grid["n_grid_y"], parts["PPD"], parts["n_particles"])
+    og = dict(n_grid=(grid["n_grid_x"], grid["n_grid_y"]), h=(dx, dx), h_nodes=(dx, grid["dy"]),
+              domain_min=(grid["domain_min_x"], grid["domain_min_y"]),
+              domain_max=(grid["domain_max_x"], grid["domain_max_y"]))
+    o = OracleEngine("coupled2d", og, x, parts["p_vol"], parts["p_rho"], parts["PPD"], mat, load,
+                     lp0=dx / parts["PPD"] / 2.0 - 1e-6, n_iter=it["n_iter"], tol=it["tol"], dt=it["dt"],
+                     phi_initial=porous["phi_initial"], mobility=porous["mobility_constant"])
+    top = o.x[:, 1] > grid["end_y"] - dx / parts["PPD"]
+    o.pbc_flag[:] = top
+    o.trac_flag[:] = top
+    return o
+
+
+def consolidation_boundary_np(boundary, n_grid_x, n_grid_y):
+    """x fixed on the side-wall node columns, y fixed on the base row."""
+    nn = (n_grid_x + 1) * (n_grid_y + 1)
+    ix = np.tile(np.arange(n_grid_x + 1), n_grid_y + 1)
+    iy = np.repeat(np.arange(n_grid_y + 1), n_grid_x + 1)
+    dof = ix + iy * (n_grid_x + 1)
+    boundary[dof[(ix <= 1) | (ix >= 2)]] = True
+    boundary[dof[iy <= 0] + nn] = True
+
+
+def oracle_consolidation_sample(dicts, dts, max_steps=20, budget_s=15.0):
+    """Seconds per load step of the full consolidation column in the oracle:
+    consecutive load steps from the start of the schedule (P2G, Newton to the
+    tolerance with a SciPy sparse direct solve, G2P) until max_steps or
+    budget_s.  Returns (seconds per step, steps run, description)."""
+    grid, parts, it, mat, porous, load = dicts
+    o = consolidation_oracle(grid, parts, it, mat, porous, load)
+    bnd = lambda b: consolidation_boundary_np(b, grid["n_grid_x"], grid["n_grid_y"])
+    t0 = time.perf_counter()
+    n = 0
+    while n < min(max_steps, len(dts)) and time.perf_counter() - t0 < budget_s:
+        o.dt = float(dts[n])
+        o.advance_one_step(n, len(dts), set_boundary=bnd)
+        n += 1
+    sec = (time.perf_counter() - t0) / n
+    desc = (f"load steps 0..{n - 1} of the full column ({o.N} particles, {o.ndof} DOFs; "
+            f"{sum(o.iters) / n:.1f} Newton iterations per step, complex-step tangents and SciPy spsolve), "
+            f"NumPy oracle on 1 host thread")
+    return sec, n, desc
