@@ -73,7 +73,7 @@ MG_MAX_LEVELS = 20
 class MgPlan(C.Structure):
     _fields_ = [("levels", C.c_int32), ("dense_n", C.c_int32), ("n_rows", C.c_int32 * MG_MAX_LEVELS),
                 ("nnzb", C.c_int32 * MG_MAX_LEVELS), ("nf", C.c_int32), ("fine_n_rows", C.c_int32),
-                ("fine_nnzb", C.c_int32), ("pad0", C.c_int32), ("workspace", C.c_void_p)]
+                ("fine_nnzb", C.c_int32), ("lag", C.c_int32), ("workspace", C.c_void_p)]
 
 
 class Adjoint(C.Structure):

@@ -879,10 +879,21 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
     for (int l = 0; l < last; ++l) {
         const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
         double *x = v.x, *y = v.x2;
-        mg_jacobi<NF, VT>(h, l, v.b, nullptr, x, 1, skip, s);
-        for (int it = 1; it < mg_sweeps(l); ++it) {
-            mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
+        if (l > 0 && mg_sweeps(l) == 2) {
+            // both zero-start sweeps in one launch, into the buffer the
+            // second separate sweep would have written
+            PtrsA a = make_ptrs(v.A);
+            const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * 8 + 4);
+            ProfScope ps(PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
+            k_mg_presmooth2<NF, double><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(
+                a, v.Minv, v.b, y, kMgOmega, skip);
             double *t = x; x = y; y = t;
+        } else {
+            mg_jacobi<NF, VT>(h, l, v.b, nullptr, x, 1, skip, s);
+            for (int it = 1; it < mg_sweeps(l); ++it) {
+                mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
+                double *t = x; x = y; y = t;
+            }
         }
         PtrsA a = make_ptrs(v.A), ca = make_ptrs(c.A);
         const double vs = 8.0 * v.A.n_rows * NF;
@@ -1051,7 +1062,9 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
             rc = mg_pattern<NF>(h, A, &local, s);
             if (rc) return rc;
         }
-        rc = mg_numeric<NF, VT>(h, s);
+        // lag: the previous solve's coarse operators, smoothers and dense
+        // inverse are still in the workspace; GMRES itself applies A
+        rc = (plan_in && plan_in->lag) ? GW_OK : mg_numeric<NF, VT>(h, s);
     }
     if (rc) return rc;
     PtrsA a = make_ptrs(*A);

@@ -340,6 +340,56 @@ __global__ void k_mg_jacobi(PtrsA A, const double *__restrict__ Minv, const doub
     }
 }
 
+// Both pre-smoothing sweeps from a zero start in one launch:
+//   x1 = omega Minv b,   x_out = x1 + omega Minv (b - A x1),
+// with the neighbours' x1 recomputed where they are read (the same
+// arithmetic as the separate zero-start sweep, so the result is bitwise the
+// same).  Used on the coarse levels, where each launch costs more than the
+// extra Minv and b reads.
+template <int NF, typename VT>
+__global__ void k_mg_presmooth2(PtrsA A, const double *__restrict__ Minv, const double *__restrict__ b,
+                                double *__restrict__ x_out, double omega, const int *__restrict__ skip) {
+    if (skip && *skip) return;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const VT *vals = (const VT *)A.vals;
+    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+        double acc[NF];
+#pragma unroll
+        for (int f = 0; f < NF; ++f) acc[f] = 0.0;
+        const int s0 = A.row_ptr[r], e0 = A.row_ptr[r + 1];
+        for (int j = s0 + lane; j < e0; j += 32) {
+            const int col = A.cols[j];
+            double t[NF], z[NF];
+#pragma unroll
+            for (int g = 0; g < NF; ++g) t[g] = b[(size_t)col * NF + g];
+            apply_minv<NF>(Minv, col, t, z);
+            const VT *blk = vals + (size_t)j * NF * NF;
+#pragma unroll
+            for (int f = 0; f < NF; ++f)
+#pragma unroll
+                for (int g = 0; g < NF; ++g) acc[f] += (double)blk[f * NF + g] * (omega * z[g]);
+        }
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) acc[f] += __shfl_down_sync(0xffffffffu, acc[f], o);
+        if (lane == 0) {
+            double t[NF], z[NF], x1[NF];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) t[f] = b[(size_t)r * NF + f];
+            apply_minv<NF>(Minv, r, t, z);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) x1[f] = omega * z[f];
+#pragma unroll
+            for (int f = 0; f < NF; ++f) t[f] = b[(size_t)r * NF + f] - acc[f];
+            apply_minv<NF>(Minv, r, t, z);
+#pragma unroll
+            for (int f = 0; f < NF; ++f) x_out[(size_t)r * NF + f] = x1[f] + omega * z[f];
+        }
+    }
+}
+
 // r = b - A x
 template <int NF, typename VT>
 __global__ void k_mg_residual(PtrsA A, const double *__restrict__ b, const double *__restrict__ x,

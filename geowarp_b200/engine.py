@@ -168,6 +168,8 @@ class Engine:
         self._R = torch.zeros(1, **f64)
         self._delta = torch.zeros(1, **f64)
         self._mg_plan = None
+        self._mg_numeric = None  # (role of the last numeric phase, its GMRES iterations)
+        self.mg_lag = True  # Newton solves of a load step share one multigrid numeric phase
         # consistent-mass system (u-p kinds)
         if self.nf > self.D:
             self.touched = torch.zeros(nn, dtype=torch.uint8, device=dev)
@@ -254,6 +256,7 @@ class Engine:
     def build_system(self):
         """Row compaction and block-CSR pattern, once per load step."""
         self._mg_plan = None  # the multigrid plan follows the pattern
+        self._mg_numeric = None
         g, s = self.grid_struct(), self.stream
         nr = C.c_int32(0)
         L.call("gw_compact_rows", C.byref(g), _p(self.node_active), _p(self.boundary), _p(self.node2row),
@@ -365,7 +368,7 @@ class Engine:
         it, rr = C.c_int32(0), C.c_double(0.0)
         rtol = rtol if rtol is not None else self.krylov_rtol
         if self.krylov_method == "gmres":
-            return self.gmres_solve(A, self._R, self._delta, rtol)
+            return self.gmres_solve(A, self._R, self._delta, rtol, newton=True)
         if self.precond == "mg":
             raise ValueError("the multigrid preconditioner runs inside GMRES (krylov='gmres')")
         else:
@@ -377,10 +380,18 @@ class Engine:
             L.check(rc, "Krylov")
         return it.value, rr.value, rc
 
-    def gmres_solve(self, A, b, x, rtol):
+    def gmres_solve(self, A, b, x, rtol, newton=False):
         """GMRES on block-CSR A (rows of this engine's active set): node-block /
         diagonal Jacobi (gw_bsr_gmres_solve) or a geometric-multigrid V-cycle
-        on the background grid (gw_bsr_gmres_mg_solve)."""
+        on the background grid (gw_bsr_gmres_mg_solve).
+
+        Multigrid: the coarse patterns are built once per load step.  With
+        mg_lag set, a Newton solve that follows another Newton solve of the
+        same load step reuses that solve's coarse operators and smoothers
+        (plan.lag); GMRES still applies the current Jacobian, so only the
+        preconditioner lags.  Any other solve (the adjoint's transpose), or a
+        lagged solve that needed more than twice the iterations of the last
+        fresh one plus five, makes the next solve rebuild them."""
         lib = L.load()
         it, rr = C.c_int32(0), C.c_double(0.0)
         if self.precond == "mg":
@@ -393,9 +404,18 @@ class Engine:
                 plan = L.MgPlan()
                 L.call("gw_mg_plan_build", C.byref(g), C.byref(A), _p(ws), ws.numel(), C.byref(plan), self.stream)
                 self._mg_plan = plan
+                self._mg_numeric = None
+            plan.lag = int(bool(self.mg_lag and newton and self._mg_numeric is not None
+                                and self._mg_numeric[0] == "newton"))
             rc = lib.gw_bsr_gmres_mg_solve(C.byref(g), C.byref(A), self.prec, C.byref(plan), _p(b), _p(x), rtol,
                                            self.krylov_max_iter, self.restart, _p(ws), ws.numel(), C.byref(it),
                                            C.byref(rr), self.stream)
+            if not newton:
+                self._mg_numeric = ("other", it.value)
+            elif not plan.lag:
+                self._mg_numeric = ("newton", it.value)
+            elif it.value > 2 * self._mg_numeric[1] + 5:
+                self._mg_numeric = None
         else:
             ws = self._kry_ws.get(lib.gw_gmres_workspace_bytes(self.n_rows, self.nf, self.restart))
             rc = lib.gw_bsr_gmres_solve(C.byref(A), self.prec, self.precond, _p(b), _p(x), rtol,

@@ -240,3 +240,57 @@ def consolidation_column_2d(precision="fp64", device=None, precond="mg", krylov_
     s.particle_pressure_boundary_flag_array[:] = top
     s.particle_traction_flag_array[:] = top
     return s, dts, cv, H
+
+
+# ---------------------------------------------------------------- 3D u-p indentation
+def indentation_3d_dicts(block_cells=(80, 80, 48), grid_cells=(96, 96, 64), dx=0.02, PPD=2, E=1e7, nu=0.3,
+                         material="Drucker-Prager", cohesion=5e3, friction_angle=30.0, dilation_angle=0.0,
+                         permeability=1e-12, viscosity=1e-3, porosity=0.5, indenter=0.4, depth=0.1, n_steps=50,
+                         dt=0.1, n_iter=10, tol=1e-9, penalty=None):
+    """Constructor dictionaries of the quarter-symmetric indentation of
+    problems/3D_indentation/3d_indentation_coupled_cpGIMP.py:11-88 at a given
+    size: a block of block_cells cells starting one cell in from the x and y
+    symmetry planes and on the base, a rigid square indenter of side
+    `indenter` on the block's corner pushed `depth` over n_steps load steps,
+    with the reference's penalty-to-modulus ratio of 1 by default."""
+    nx, ny, nz = grid_cells
+    sx, sy, sz = dx, dx, 0.0
+    ex, ey, ez = sx + block_cells[0] * dx, sy + block_cells[1] * dx, sz + block_cells[2] * dx
+    grid = dict(n_grid_x=nx, n_grid_y=ny, n_grid_z=nz, max_x=nx * dx, dx=dx, max_y=ny * dx, dy=dx, max_z=nz * dx,
+                dz=dx, start_x=sx, end_x=ex, start_y=sy, end_y=ey, start_z=sz, end_z=ez, domain_min_x=sx,
+                domain_max_x=ex, domain_min_y=sy, domain_max_y=ey, domain_min_z=sz, domain_max_z=nz * dx)
+    n = block_cells[0] * block_cells[1] * block_cells[2] * PPD ** 3
+    parts = dict(n_particles=n, PPD=PPD, p_vol=(dx / PPD) ** 3, p_rho=2.0)
+    it = dict(n_iter=n_iter, tol=tol, solver_name="scipy", dt=dt)
+    mat = dict(youngs_modulus=E, poisson_ratio=nu, material_name=material)
+    if material == "Drucker-Prager":
+        mat.update(friction_angle=friction_angle, dilation_angle=dilation_angle, cohesion=cohesion, shape_factor=0.0,
+                   tension_cutoff=False)
+    porous = dict(phi_initial=porosity, mobility_constant=permeability / viscosity)
+    load = dict(gravity_mag=0.0, traction_value_x=0.0, traction_value_y=0.0, traction_value_z=0.0,
+                point_load_value_x=0.0, point_load_value_y=0.0, point_load_value_z=0.0,
+                footing_region_min_x=sx, footing_region_max_x=sx + indenter, footing_region_min_y=sy,
+                footing_region_max_y=sy + indenter, footing_initial_height=ez - dx / PPD,
+                footing_incr_disp=-depth / n_steps, penalty_factor=E if penalty is None else penalty)
+    return grid, parts, it, mat, porous, load
+
+
+def indentation_boundary_dofs(tid, boundary_flag_array, n_grid_x, n_grid_y, n_nodes, dx, dy, end_x, end_y):
+    """set_boundary_dofs of 3d_indentation_coupled_cpGIMP.py:126-153 on index
+    tensors: rollers on the symmetry planes and the far walls, fixed base."""
+    ix, iy, iz = tid
+    dof_x = ix + iy * (n_grid_x + 1) + iz * ((n_grid_x + 1) * (n_grid_y + 1))
+    boundary_flag_array[dof_x[(ix <= 1) | ((ix + 0.5) * dx > end_x)]] = True
+    boundary_flag_array[(dof_x + n_nodes)[(iy <= 1) | ((iy + 0.5) * dy > end_y)]] = True
+    boundary_flag_array[(dof_x + 2 * n_nodes)[iz <= 0]] = True
+
+
+def indentation_3d(precision="fp64", device=None, precond="mg", **kw):
+    """The 3D coupled u-p indentation (keywords of indentation_3d_dicts),
+    drained top surface (set_pressure_boundary of the reference script)."""
+    from .solvers.quasi_static_coupled_solver_3d import quasi_static_coupled_solver_3d
+    grid, parts, it, mat, porous, load = indentation_3d_dicts(**kw)
+    s = quasi_static_coupled_solver_3d(grid, parts, it, mat, porous, load, indentation_boundary_dofs,
+                                       precision=precision, device=device, precond=precond)
+    s.particle_pressure_boundary_flag_array[:] = s.x_particles[:, 2] > grid["end_z"] - grid["dz"] / parts["PPD"]
+    return s

@@ -289,14 +289,22 @@ int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const d
  * gw_bsr_gmres_mg_solve: the numeric phase (Galerkin values, smoothers, dense
  * inverse; no host reads) and the solve.  plan_host == NULL builds a plan
  * first.  workspace: at least gw_gmres_mg_workspace_bytes(grid, n_rows, nf,
- * restart) bytes (the plan needs the hierarchy part, which comes first). */
+ * restart) bytes (the plan needs the hierarchy part, which comes first).
+ * With plan_host->lag = 1 the numeric phase is skipped: the V-cycle reuses the
+ * coarse operators, smoother blocks and coarsest inverse left in the
+ * workspace by the previous solve with this plan (a matrix of the same
+ * pattern and role, e.g. the previous Newton iterate's Jacobian), while
+ * GMRES applies A itself, so the solution is A's; only the preconditioner
+ * lags.  The caller must have run one solve with lag = 0 on this plan and
+ * workspace first. */
 #define GW_MG_MAX_LEVELS 20
 typedef struct gw_mg_plan {
     int32_t levels;                     /* levels holding a matrix; the last one is solved densely */
     int32_t dense_n;                    /* unknowns of the coarsest level                          */
     int32_t n_rows[GW_MG_MAX_LEVELS];
     int32_t nnzb[GW_MG_MAX_LEVELS];
-    int32_t nf, fine_n_rows, fine_nnzb, pad0;
+    int32_t nf, fine_n_rows, fine_nnzb;
+    int32_t lag;                        /* 1: reuse the previous solve's numeric phase (see above)  */
     const void *workspace;              /* the coarse patterns live in this workspace              */
 } gw_mg_plan_t;
 int64_t gw_gmres_mg_workspace_bytes(const gw_grid_t *grid, int32_t n_rows, int32_t nf, int32_t restart);
