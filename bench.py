@@ -15,7 +15,7 @@ collective) and `value` is the aggregate over ranks.
 --workload batched runs 64 inverse-analysis blocks packed into one engine;
 --workload consolidation runs the 1 x 200-cell coupled u-p column (forward
 load steps with their own time increments; the adjoint covers the 2D solid
-solver).
+solver); --workload bar runs the 4 x 40-cell self-weight bar.
 
 --impl reference times the CPU restatement of the reference's algorithm (the
 reference itself runs only on NVIDIA Warp, not installable here) on a bounded
@@ -51,9 +51,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geowarp", choices=["geowarp", "reference"])
     ap.add_argument("--small", action="store_true", help="64x32-cell variant for quick checks")
-    ap.add_argument("--workload", default="footing", choices=["footing", "batched", "consolidation"],
+    ap.add_argument("--workload", default="footing", choices=["footing", "batched", "consolidation", "bar"],
                     help="footing: the strip footing (default); batched: 64 inverse-analysis blocks in one engine; "
-                         "consolidation: the 1 x 200-cell u-p column (forward load steps)")
+                         "consolidation: the 1 x 200-cell u-p column (forward load steps); bar: the 4 x 40-cell "
+                         "self-weight bar")
     ap.add_argument("--instances", type=int, default=64, help="blocks of the batched workload")
     ap.add_argument("--profile", action="store_true", help="also time the dominant kernel (instrumented pass)")
     ap.add_argument("--ncu", action="store_true",
@@ -67,25 +68,42 @@ def footing_kwargs(small):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed
+    region: sampling starts (and its first row is awaited) before the region,
+    every row carries its timestamp, and only rows inside [mark_start,
+    mark_end] are summarised (the nearest row when the region is shorter than
+    the sampling interval, flagged as such)."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    PERIOD_MS = 25
 
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
+        self.t0 = self.t1 = None
 
     def __enter__(self):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+                                          "--format=csv,noheader,nounits", "-lms", str(self.PERIOD_MS)],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        if self.proc is not None:
+            deadline = time.time() + 5.0
+            while time.time() < deadline and not os.path.getsize(self.f.name):
+                time.sleep(0.02)
         return self
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
+        time.sleep(2.0 * self.PERIOD_MS / 1e3)  # let the row that covers the end arrive
 
     def __exit__(self, *a):
         if self.proc is not None:
@@ -95,23 +113,44 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
+    @staticmethod
+    def _when(stamp):
+        import datetime
+        try:
+            return datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def summary(self):
         try:
             rows = [l.split(",") for l in open(self.f.name).read().strip().split("\n") if l.strip()]
         except OSError:
             rows = []
         os.unlink(self.f.name)
+        rows = [r for r in rows if len(r) >= 10]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows]
+        timed = [(self._when(r[0]), r) for r in rows]
+        note = None
+        if self.t0 is not None and self.t1 is not None and all(t is not None for t, _ in timed):
+            inside = [r for t, r in timed if self.t0 <= t <= self.t1]
+            if not inside:
+                mid = 0.5 * (self.t0 + self.t1)
+                inside = [min(timed, key=lambda tr: abs(tr[0] - mid))[1]]
+                note = "timed region shorter than the sampling interval: nearest sample"
+            rows = inside
+        sm = [float(r[2]) for r in rows]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
-            for name, v in zip(names, r[5:9]):
+            for name, v in zip(names, r[6:10]):
                 if v.strip() == "Active":
                     reasons.add(name)
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
-                "samples": len(rows)}
+        out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][3]), "reasons": sorted(reasons),
+               "samples": len(rows), "period_ms": self.PERIOD_MS}
+        if note:
+            out["note"] = note
+        return out
 
 
 # ------------------------------------------------------------------ workloads
@@ -199,6 +238,33 @@ class BatchedWorkload(Workload):
         return {}
 
 
+class BarWorkload(Workload):
+    """Self-weight bar: 4 x 40 cells of 0.25 m, 2 x 2 particles per cell,
+    compressible neo-Hookean; forward + adjoint load steps."""
+
+    def __init__(self, args):
+        self.units = 1
+        self.n_steps = 50
+        self.config = dict(workload="2D quasi-static bar compaction under self-weight",
+                           cells="4x40 cells (8x44 grid), dx=0.25 m", particles=640, ppc="2x2",
+                           material="compressible neo-Hookean E=1e6 Pa nu=0.3 rho=80 kg/m3",
+                           load="gravity 9.81 ramped over 50 load steps; roller side walls, fixed base",
+                           newton="||R|| < 1e-6 N (1e-8 of one step's load increment)")
+        self.metric = METRIC
+
+    def make(self, precision, dev):
+        from geowarp_b200 import problems
+        from geowarp_b200.adjoint import LoadStepAdjoint
+        s = problems.bar_compaction_2d(precision=precision, device=dev)
+        return s, LoadStepAdjoint(s)
+
+    def seed(self, adj, k):
+        adj.seed_displacement_misfit()
+
+    def errors(self, s_mx, s_64):
+        return {}
+
+
 class ConsolidationStepper:
     """Forward load steps of the consolidation column, each with its own time
     increment."""
@@ -252,6 +318,8 @@ def make_workload(args):
         return BatchedWorkload(args)
     if args.workload == "consolidation":
         return ConsolidationWorkload(args)
+    if args.workload == "bar":
+        return BarWorkload(args)
     return FootingWorkload(args)
 
 
@@ -293,12 +361,14 @@ def run_geowarp(args):
     with ClockSampler(dev.index) as cs:
         sync()
         n_launch0 = lib.gw_launch_count()
+        cs.mark_start()
         ev0.record()
         for k in range(W, W + K):
             l2_flush.zero_()
             one_step(adj_mx, k)
         ev1.record()
         sync()
+        cs.mark_end()
         launches = lib.gw_launch_count() - n_launch0
     ms_mx = ev0.elapsed_time(ev1)
     clocks = cs.summary()
@@ -427,6 +497,11 @@ def cpu_baseline(wl, gpu_line):
         from oracle.bench_sample import oracle_consolidation_sample
         sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts)
         return {"value": 1.0 / sec, "unit": gpu_line["unit"], "cores": 1, "kind": "port", "sample": sample}
+    if isinstance(wl, BarWorkload):
+        from oracle.bench_sample import oracle_bar_sample
+        sec, n, sample = oracle_bar_sample(wl.n_steps)
+        return {"value": 1.0 / sec, "unit": gpu_line["unit"], "cores": 1, "kind": "port",
+                "sample": sample + " (forward load steps; the CPU path has no adjoint)"}
     from oracle.bench_sample import oracle_load_step_sample
     sec, its, sample = oracle_load_step_sample()
     scale = 1.0
@@ -453,6 +528,11 @@ def run_reference(args):
         from oracle.bench_sample import oracle_consolidation_sample
         sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts, max_steps=max(args.steps, 3),
                                                      budget_s=60.0)
+        v = 1.0 / sec
+    elif isinstance(wl, BarWorkload):
+        from oracle.bench_sample import oracle_bar_sample
+        sec, n, sample = oracle_bar_sample(wl.n_steps, max_steps=max(args.steps, 3), budget_s=60.0)
+        sample += " (forward load steps; the CPU path has no adjoint)"
         v = 1.0 / sec
     else:
         from oracle.bench_sample import oracle_load_step_sample

@@ -879,14 +879,19 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
     for (int l = 0; l < last; ++l) {
         const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
         double *x = v.x, *y = v.x2;
-        if (l > 0 && mg_sweeps(l) == 2) {
+        if (mg_sweeps(l) == 2) {
             // both zero-start sweeps in one launch, into the buffer the
             // second separate sweep would have written
             PtrsA a = make_ptrs(v.A);
-            const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * 8 + 4);
-            ProfScope ps(PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
-            k_mg_presmooth2<NF, double><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(
-                a, v.Minv, v.b, y, kMgOmega, skip);
+            const double vs = 8.0 * v.A.n_rows * NF;
+            const double mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
+            ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
+            if (l == 0)
+                k_mg_presmooth2<NF, VT><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(
+                    a, v.Minv, v.b, y, kMgOmega, skip);
+            else
+                k_mg_presmooth2<NF, double><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(
+                    a, v.Minv, v.b, y, kMgOmega, skip);
             double *t = x; x = y; y = t;
         } else {
             mg_jacobi<NF, VT>(h, l, v.b, nullptr, x, 1, skip, s);

@@ -12,7 +12,7 @@
 //   coarse operator: Galerkin A_{l+1} = P^T A_l P in the same 5^D-stencil
 //     block-CSR layout (a coarse block (I,J) gathers the fine blocks (i,j) of
 //     I's and J's children in a fixed order: deterministic, no atomics);
-//   smoother: damped node-block Jacobi; coarsest level (at most 40 unknowns):
+//   smoother: damped node-block Jacobi; coarsest level (at most 160 unknowns):
 //     explicit dense inverse.
 //
 // Coupled u-p systems (D displacement fields and one pressure field per node)
@@ -34,7 +34,9 @@
 namespace gw {
 
 constexpr int kMgMaxLevels = GW_MG_MAX_LEVELS;
-constexpr int kMgCoarseMax = 40;  // unknowns of the coarsest (dense) level
+// unknowns of the coarsest (dense) level: its n x n FP64 matrix (204,800 bytes
+// at 160) is inverted in one CTA's shared memory
+constexpr int kMgCoarseMax = 160;
 
 // lattice node counts of a grid (cells + 1 per axis; 1 on unused axes)
 struct Lat {
@@ -344,8 +346,8 @@ __global__ void k_mg_jacobi(PtrsA A, const double *__restrict__ Minv, const doub
 //   x1 = omega Minv b,   x_out = x1 + omega Minv (b - A x1),
 // with the neighbours' x1 recomputed where they are read (the same
 // arithmetic as the separate zero-start sweep, so the result is bitwise the
-// same).  Used on the coarse levels, where each launch costs more than the
-// extra Minv and b reads.
+// same).  The extra Minv and b reads of the neighbours stay in L2; the
+// launch and the round trip of x1 through memory are saved.
 template <int NF, typename VT>
 __global__ void k_mg_presmooth2(PtrsA A, const double *__restrict__ Minv, const double *__restrict__ b,
                                 double *__restrict__ x_out, double omega, const int *__restrict__ skip) {

@@ -277,7 +277,7 @@ int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const d
  * factor-2 coarsening per axis, Galerkin coarse operators P^T A P in the same
  * block-CSR layout (FP64), two damped node-block-Jacobi sweeps before and after
  * each coarse correction, an explicit dense inverse on the coarsest level
- * (<= 40 unknowns).  Identity rows of A (Dirichlet DOFs) are excluded from the
+ * (<= 160 unknowns).  Identity rows of A (Dirichlet DOFs) are excluded from the
  * transfer operators.
  *
  * gw_mg_plan_build: the pattern phase (coarse active sets, stencils, block-CSR

@@ -175,3 +175,45 @@ def oracle_consolidation_sample(dicts, dts, max_steps=20, budget_s=15.0):
             f"{sum(o.iters) / n:.1f} Newton iterations per step, complex-step tangents and SciPy spsolve), "
             f"NumPy oracle on 1 host thread")
     return sec, n, desc
+
+
+def bar_oracle(width_cells=4, height_cells=40, dx=0.25, PPD=2, E=1e6, nu=0.3, rho=80.0, gravity=9.81,
+               material="Neo-Hookean", n_iter=20, tol=1e-6):
+    """The self-weight bar (problems/bar_compaction/bar_compaction_cpGIMP.py
+    layout in SI units): rollers on both side walls, fixed base, two empty
+    cells around the bar, gravity ramped over the load steps."""
+    pad = 2
+    n_grid_x, n_grid_y = width_cells + 2 * pad, height_cells + 2 * pad
+    sx, sy = pad * dx, pad * dx
+    ex, ey = sx + width_cells * dx, sy + height_cells * dx
+    x = init_particles_rectangle_2d(sx, sy, ex, ey, dx, n_grid_x, n_grid_y, PPD, width_cells * height_cells * PPD * PPD)
+    mat = dict(youngs_modulus=E, poisson_ratio=nu, material_name=material)
+    load = dict(gravity_mag=gravity, traction_value_x=0.0, traction_value_y=0.0, point_load_value_x=0.0,
+                point_load_value_y=0.0)
+    grid = dict(n_grid=(n_grid_x, n_grid_y), h=(dx, dx), h_nodes=(dx, dx), domain_min=(sx, sy), domain_max=(ex, ey))
+    o = OracleEngine("solid2d", grid, x, (dx / PPD) ** 2, rho, PPD, mat, load, lp0=dx / PPD / 2.0 - 1e-6,
+                     n_iter=n_iter, tol=tol)
+    nn = (n_grid_x + 1) * (n_grid_y + 1)
+    ix = np.tile(np.arange(n_grid_x + 1), n_grid_y + 1)
+    iy = np.repeat(np.arange(n_grid_y + 1), n_grid_x + 1)
+    o.boundary[((ix <= pad) | (ix >= pad + width_cells)).nonzero()[0]] = True
+    o.boundary[(iy <= pad).nonzero()[0]] = True
+    o.boundary[(iy <= pad).nonzero()[0] + nn] = True
+    return o
+
+
+def oracle_bar_sample(n_steps=50, max_steps=50, budget_s=15.0):
+    """Seconds per load step of the self-weight bar in the oracle:
+    consecutive load steps from the start (P2G, Newton with a SciPy sparse
+    direct solve, G2P) until max_steps or budget_s.  Returns (seconds per
+    step, steps run, description)."""
+    o = bar_oracle()
+    t0 = time.perf_counter()
+    n = 0
+    while n < min(max_steps, n_steps) and time.perf_counter() - t0 < budget_s:
+        o.advance_one_step(n, n_steps)
+        n += 1
+    sec = (time.perf_counter() - t0) / n
+    desc = (f"load steps 0..{n - 1} of the bar ({o.N} particles, {o.ndof} DOFs; {sum(o.iters) / n:.1f} Newton "
+            f"iterations per step, complex-step tangents and SciPy spsolve), NumPy oracle on 1 host thread")
+    return sec, n, desc
