@@ -135,11 +135,14 @@ SIGNATURES = {
 _lib = None
 
 
-def load(path=LIB):
-    """Load the shared library (raises if it is missing)."""
+def load(path=None):
+    """Load the shared library (raises if it is missing).  The environment
+    variable GEOWARP_B200_LIB names another build of it (a variant compiled for
+    an A/B timing); the default is the in-tree library."""
     global _lib
     if _lib is not None:
         return _lib
+    path = path or os.environ.get("GEOWARP_B200_LIB") or LIB
     if not os.path.exists(path):
         raise RuntimeError(f"{path} is missing: run geowarp_b200.build.build() (the engine has no CPU fallback)")
     lib = C.CDLL(path)

@@ -1428,8 +1428,18 @@ extern "C" int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, c
     LaunchConst c = make_lc(grid, mat, st);
     c.mc.tip_tangent = 0.0;  // exact derivatives of the converged state
     ProfScope ps(PC_ADJ_G2P, s, (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 18 + 23 + 2 * 9 * 2));
-    k_adjoint_g2p<<<gw_count_launch(nblk(pt->n, 128)), 128, 0, s>>>(c, make_ptrs(*pt), u_new, u_old, free_mask, make_ptrs(*A),
-                                                 make_adj(*seed_in), make_adj(*q_out), ubar_rows);
+    const dim3 grd(gw_count_launch(nblk(pt->n, 128))), blk(128);
+    const PtrsP pp = make_ptrs(*pt);
+    const PtrsA pa = make_ptrs(*A);
+    const AdjState si = make_adj(*seed_in), qo = make_adj(*q_out);
+    switch (mat->model) {  // one instantiation per material: see solid2d_dual
+        case GW_MODEL_HENCKY: k_adjoint_g2p<GW_MODEL_HENCKY><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
+        case GW_MODEL_J2: k_adjoint_g2p<GW_MODEL_J2><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
+        case GW_MODEL_DP: k_adjoint_g2p<GW_MODEL_DP><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
+        case GW_MODEL_NEOHOOKEAN: k_adjoint_g2p<GW_MODEL_NEOHOOKEAN><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
+        case GW_MODEL_LINEAR: k_adjoint_g2p<GW_MODEL_LINEAR><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
+        default: k_adjoint_g2p<-1><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
+    }
     GW_LAUNCHED();
     return GW_OK;
 }
@@ -1445,8 +1455,19 @@ extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *m
     LaunchConst c = make_lc(grid, mat, st);
     c.mc.tip_tangent = 0.0;  // exact derivatives of the converged residual
     ProfScope ps(PC_ADJ_RES, S(stream), (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 23 * 2 + 2 * 9 * 2 + 9 * 2));
-    k_adjoint_residual<<<gw_count_launch(nblk(pt->n, 128)), 128, 0, S(stream)>>>(c, make_ptrs(*pt), u_new, u_old, free_mask,
-                                                                make_ptrs(*A), lambda_rows, make_adj(*q_out));
+    const dim3 grd(gw_count_launch(nblk(pt->n, 128))), blk(128);
+    const PtrsP pp = make_ptrs(*pt);
+    const PtrsA pa = make_ptrs(*A);
+    const AdjState qo = make_adj(*q_out);
+    cudaStream_t s = S(stream);
+    switch (mat->model) {  // one instantiation per material: see solid2d_dual
+        case GW_MODEL_HENCKY: k_adjoint_residual<GW_MODEL_HENCKY><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
+        case GW_MODEL_J2: k_adjoint_residual<GW_MODEL_J2><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
+        case GW_MODEL_DP: k_adjoint_residual<GW_MODEL_DP><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
+        case GW_MODEL_NEOHOOKEAN: k_adjoint_residual<GW_MODEL_NEOHOOKEAN><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
+        case GW_MODEL_LINEAR: k_adjoint_residual<GW_MODEL_LINEAR><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
+        default: k_adjoint_residual<-1><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
+    }
     GW_LAUNCHED();
     return GW_OK;
 }

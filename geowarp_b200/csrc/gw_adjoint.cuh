@@ -100,7 +100,11 @@ struct SolidDual {
 };
 
 // Forward pass of one 2D solid particle in dual arithmetic.  du: nodal
-// increments of the 9 slots (u_new - u_old), values only.
+// increments of the 9 slots (u_new - u_old), values only.  MODEL is the
+// material (GW_MODEL_*) fixed at compile time, so an instantiation carries
+// only its own constitutive code (the return maps in 19-lane duals dominate
+// the stack frame); MODEL < 0 reads it from c at run time.
+template <int MODEL>
 GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lpv, const double *Fo_v,
                              const double *bo_v, double Ev, const double fext[2], const double du[9][2], bool want_g2p,
                              SolidDual &o) {
@@ -163,7 +167,7 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
 
     // stress (Kirchhoff) and b_new
     AD tau[3][3];
-    const int model = c.mc.model;
+    const int model = MODEL >= 0 ? MODEL : c.mc.model;
     if (model == GW_MODEL_HENCKY || model == GW_MODEL_J2 || model == GW_MODEL_DP) {
         double B[3][3], lamb[3], V[3][3];
         for (int i = 0; i < 3; ++i)
@@ -277,6 +281,7 @@ struct AdjState {  // per-particle adjoint arrays (user order)
 
 // Adjoint G2P: seeds (x_new, lp_new, F_new, b_new) bars -> q_bar (written) and
 // the nodal adjoint u_bar (free DOFs of active rows, atomically accumulated).
+template <int MODEL>
 __global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__ u_new,
                               const double *__restrict__ u_old, const uint8_t *__restrict__ free_mask, PtrsA A,
                               AdjState seed_in, AdjState q_out, double *__restrict__ ubar_rows) {
@@ -298,7 +303,7 @@ __global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
     const bool ext = p.ext_flag && p.ext_flag[pid];
     const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
-    solid2d_dual(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
+    solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
                  true, o);
     AD s(0.0);
     double xb_eff[2];
@@ -337,6 +342,7 @@ __global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__
 }
 
 // Adjoint P2G: q_bar += sum_a lambda_a . d r_a / d q over free DOFs.
+template <int MODEL>
 __global__ void k_adjoint_residual(LaunchConst c, PtrsP p, const double *__restrict__ u_new,
                                    const double *__restrict__ u_old, const uint8_t *__restrict__ free_mask, PtrsA A,
                                    const double *__restrict__ lambda_rows, AdjState q_out) {
@@ -358,7 +364,7 @@ __global__ void k_adjoint_residual(LaunchConst c, PtrsP p, const double *__restr
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
     const bool ext = p.ext_flag && p.ext_flag[pid];
     const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
-    solid2d_dual(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
+    solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
                  false, o);
     AD s(0.0);
     for (int a = 0; a < 9; ++a) {
