@@ -344,6 +344,19 @@ extern "C" int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_
 
 // ==================================================================== residual + Jacobian
 namespace {
+template <int KIND, typename VT>
+void assemble_per_model(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
+                        const double *uo, const PtrsA &a, double *R, double *force, int b, cudaStream_t s) {
+    switch (c.mc.model) {
+        case GW_MODEL_HENCKY: k_assemble<KIND, true, VT, GW_MODEL_HENCKY><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_J2: k_assemble<KIND, true, VT, GW_MODEL_J2><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_NEOHOOKEAN: k_assemble<KIND, true, VT, GW_MODEL_NEOHOOKEAN><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_LINEAR: k_assemble<KIND, true, VT, GW_MODEL_LINEAR><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_DP: k_assemble<KIND, true, VT, GW_MODEL_DP><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        default: k_assemble<KIND, true, VT><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+    }
+}
+
 template <int KIND>
 int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
                     const double *uo, const gw_bsr_t *A, int prec, double *R, double *force, const PtrsA &a,
@@ -360,9 +373,17 @@ int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const
         const bool want_K = A->vals != nullptr;
         const double mat = want_K ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
         ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + grid + mat);
-        if (!want_K) k_assemble<KIND, false, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-        else if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-        else k_assemble<KIND, true, float><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        if (!want_K) {
+            k_assemble<KIND, false, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        } else if constexpr (KIND == GW_KIND_SOLID2D) {
+            // the 2D solid tangent kernel is instantiated per material, so each
+            // carries only its own constitutive code (fewer registers and spills)
+            if (prec == GW_PREC_F64) assemble_per_model<KIND, double>(c, p, perm, fm, un, uo, a, R, force, b, s);
+            else assemble_per_model<KIND, float>(c, p, perm, fm, un, uo, a, R, force, b, s);
+        } else {
+            if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+            else k_assemble<KIND, true, float><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+        }
         GW_LAUNCHED();
     }
     if (A->vals && A->n_rows > 0) {

@@ -196,7 +196,7 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
         tau_hencky(e, lam, mu, tA);
         // coalescence limits from the value-level algorithmic tangent
         double tv[3], dtau[3][4], ev[3], de[3][4], pn = 0.0;
-        principal_model<double>(c.mc, lam.v, mu.v, etr_v, 0.0, 0.0, pn, tv, dtau, ev, true, de);
+        principal_model<double, MODEL>(c.mc, lam.v, mu.v, etr_v, 0.0, 0.0, pn, tv, dtau, ev, true, de);
         double limT[3][3], limB[3][3];
         AD fB[3];
         for (int A = 0; A < 3; ++A) {

@@ -290,7 +290,9 @@ GW_HD void tau_norsand(const T e[3], const MatConst &c, T tau[3]) {
 // Principal model with its algorithmic tangent: lanes 0..2 seed e_trial_B,
 // lane 3 seeds the total volumetric strain (NorSand's specific volume).
 // Outputs tau[A], dtau[A][lane], e_out[A]; pi_new updated for plastic NorSand.
-template <typename R>
+// MODEL (GW_MODEL_*) fixed at compile time drops the other models' code from
+// the caller's instantiation; MODEL < 0 dispatches on c.model at run time.
+template <typename R, int MODEL = -1>
 GW_HD void principal_model(const MatConst &c, R lam, R mu, const R etr_v[3], R eps_v_total, R pi_old, R &pi_new,
                            R tau_v[3], R dtau[3][4], R e_out[3], bool want_tangent, R (*de)[4] = nullptr) {
     typedef Dual<4, R> T;
@@ -302,7 +304,7 @@ GW_HD void principal_model(const MatConst &c, R lam, R mu, const R etr_v[3], R e
     }
     T evt = T(eps_v_total);
     if (want_tangent) evt.d[3] = R(1);
-    switch (c.model) {
+    switch (MODEL >= 0 ? MODEL : c.model) {
         case GW_MODEL_J2:
             rm_j2<T, R, R>(etr, lam, mu, R(c.kappa), e);
             tau_hencky(e, lam, mu, tau);

@@ -179,14 +179,14 @@ GW_HD void spectral_dtau(const double lamb[3], const double V[3][3], const doubl
         for (int j = 0; j < 3; ++j) dtau_out[i][j] = T1[i][0] * V[j][0] + T1[i][1] * V[j][1] + T1[i][2] * V[j][2];
 }
 
-template <int KIND, bool TANGENT>
+template <int KIND, bool TANGENT, int MODEL = -1>
 GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const double *xp,
                                               const double *F_old, const double *b_old, double E, double pi_old,
                                               double pi_new_in, double V0, PEval<KIND> &ev) {
     const int D = KindTraits<KIND>::D;
     const bool UP = KindTraits<KIND>::UP;
     typedef Layout<KIND> L;
-    const int model = c.mc.model;
+    const int model = MODEL >= 0 ? MODEL : c.mc.model;
     const double nu = c.nu;
     ev.lam = E * nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
     ev.mu = E / (2.0 * (1.0 + nu));
@@ -229,7 +229,7 @@ GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const doub
         for (int A = 0; A < 3; ++A) etr[A] = 0.5 * ::log(fmax(lamb[A], 1e-8));
         const double evt = ::log(J) + c.mc.ns_ev0;
         double pn = ev.pi_new;
-        principal_model<double>(c.mc, ev.lam, ev.mu, etr, evt, pi_old, pn, tauA, dtau, e, TANGENT);
+        principal_model<double, MODEL>(c.mc, ev.lam, ev.mu, etr, evt, pi_old, pn, tauA, dtau, e, TANGENT);
         ev.pi_new = pn;
         for (int i = 0; i < 3; ++i)
             for (int j = 0; j < 3; ++j) {

@@ -300,7 +300,7 @@ __global__ void k_pattern_fill(gw_grid_t g, PtrsA A, int *__restrict__ cols) {
 }
 
 // ================================================================ residual + element tangent
-template <int KIND, bool WANT_K, typename VT>
+template <int KIND, bool WANT_K, typename VT, int MODEL = -1>
 __global__ void __launch_bounds__(kThreads) k_assemble(LaunchConst c, PtrsP p, const int *__restrict__ perm,
                                                        const uint8_t *__restrict__ free_mask,
                                                        const double *__restrict__ u_new,
@@ -324,7 +324,7 @@ __global__ void __launch_bounds__(kThreads) k_assemble(LaunchConst c, PtrsP p, c
     if (!particle_shape<KIND>(c.g, x, lp, s)) atomicOr(&g_status, ST_RANGE);
     particle_gather<KIND>(u_new, u_old, s);
     PEval<KIND> ev;
-    particle_eval<KIND, WANT_K>(c, s, x, Fo, bo, E, pi_old, pi_new, V0, ev);
+    particle_eval<KIND, WANT_K, MODEL>(c, s, x, Fo, bo, E, pi_old, pi_new, V0, ev);
 
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
