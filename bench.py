@@ -57,6 +57,8 @@ def parse():
                          "self-weight bar")
     ap.add_argument("--instances", type=int, default=64, help="blocks of the batched workload")
     ap.add_argument("--profile", action="store_true", help="also time the dominant kernel (instrumented pass)")
+    ap.add_argument("--autotune", default="on", choices=["on", "off"],
+                    help="search the library's launch-shape knobs on this workload before timing (untimed)")
     ap.add_argument("--ncu", action="store_true",
                     help="run warmup + steps load steps (fwd+adjoint, mixed) with no timing: the command profiled by ncu")
     return ap.parse_args()
@@ -357,6 +359,8 @@ def run_geowarp(args):
     for k in range(W):
         one_step(adj_mx, k)
     sync()
+    tuned = autotune_workload(wl, s_mx, adj_mx, W) if args.autotune == "on" else None
+    sync()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as cs:
         sync()
@@ -460,10 +464,43 @@ def run_geowarp(args):
             "newton": newton,
             "roofline": roof,
             "clocks": clocks,
+            "autotune": tuned,
         }
         line["cpu_baseline"] = cpu_baseline(wl, line)
         print(json.dumps(line))
     rep.close()
+
+
+def autotune_workload(wl, solver, adj, k):
+    """Search the launch-shape knobs (geowarp_b200.autotune) on load step k of
+    this workload: every trial restores the particle and adjoint state taken
+    after the warm-up and runs the same step, so all candidates do the same
+    work.  The state and the Newton log are restored afterwards; the chosen
+    knobs stay set for every timed arm."""
+    from geowarp_b200 import autotune
+    e = solver.engine
+    snap = autotune.snapshot(e)
+    adj_t = []
+    if getattr(adj, "grad_E", None) is not None:
+        adj_t = [adj.grad_E] + list(adj.bar.values()) + list(adj.q.values())
+    adj_snap = [t.clone() for t in adj_t]
+    n_log = len(e.log)
+
+    def reset():
+        autotune.restore(e, snap)
+        for t, c in zip(adj_t, adj_snap):
+            t.copy_(c)
+
+    def trial():
+        reset()
+        wl.step(adj, k)
+
+    best, table = autotune.tune(trial, reps=2)
+    reset()
+    del e.log[n_log:]
+    return {"config": best, "median_ms": {n: {str(c): round(v, 3) for c, v in t.items()} for n, t in table.items()},
+            "trial": f"load step {k} ({'forward + adjoint' if wl.adjoint else 'forward'}) from a restored state; "
+                     "median of 2 after an untimed call; coordinate search in the listed order"}
 
 
 def newton_stats(engine):

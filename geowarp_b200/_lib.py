@@ -16,6 +16,7 @@ MODEL_HENCKY, MODEL_J2, MODEL_NEOHOOKEAN, MODEL_LINEAR, MODEL_DP, MODEL_NORSAND 
 PREC_F64, PREC_F32 = 0, 1
 PRECOND_DIAG, PRECOND_BLOCK = 0, 1
 KRYLOV_BICGSTAB, KRYLOV_CG, KRYLOV_GMRES = 0, 1, 2
+TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_COUNT = 0, 1, 2, 3, 4
 
 
 class GeoWarpError(RuntimeError):
@@ -122,6 +123,8 @@ SIGNATURES = {
     "gw_profile_enable": (C.c_int, [I32]),
     "gw_profile_count": (C.c_int, []),
     "gw_launch_count": (I64, []),
+    "gw_tune_set": (C.c_int, [I32, I32]),
+    "gw_tune_get": (I32, [I32]),
     "gw_profile_reset": (C.c_int, []),
     "gw_profile_read": (C.c_int, [I32, PD, C.POINTER(C.c_int64), PD]),
     "gw_profile_name": (C.c_char_p, [I32]),

@@ -84,6 +84,15 @@ inline int gw_count_launch(int grid) {
     return grid;
 }
 inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+// launch-shape knobs (gw_tune_set): particle CTA, adjoint CTA, warps per CTA
+// of the multigrid row kernels, bound of the dense coarsest level
+int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160};
+inline int tune_rows_grid(int n_rows) {
+    const int w = g_tune[GW_TUNE_ROW_WARPS];
+    int b = nblk(n_rows, w);
+    return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b);
+}
+inline int tune_rows_block() { return 32 * g_tune[GW_TUNE_ROW_WARPS]; }
 inline int red_grid_rows(int n_rows) { int b = nblk(n_rows, kThreads / 32); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
 inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
 
@@ -347,13 +356,14 @@ namespace {
 template <int KIND, typename VT>
 void assemble_per_model(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
                         const double *uo, const PtrsA &a, double *R, double *force, int b, cudaStream_t s) {
+    const int pb = g_tune[GW_TUNE_PARTICLE_BLOCK];
     switch (c.mc.model) {
-        case GW_MODEL_HENCKY: k_assemble<KIND, true, VT, GW_MODEL_HENCKY><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_J2: k_assemble<KIND, true, VT, GW_MODEL_J2><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_NEOHOOKEAN: k_assemble<KIND, true, VT, GW_MODEL_NEOHOOKEAN><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_LINEAR: k_assemble<KIND, true, VT, GW_MODEL_LINEAR><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_DP: k_assemble<KIND, true, VT, GW_MODEL_DP><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        default: k_assemble<KIND, true, VT><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_HENCKY: k_assemble<KIND, true, VT, GW_MODEL_HENCKY><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_J2: k_assemble<KIND, true, VT, GW_MODEL_J2><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_NEOHOOKEAN: k_assemble<KIND, true, VT, GW_MODEL_NEOHOOKEAN><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_LINEAR: k_assemble<KIND, true, VT, GW_MODEL_LINEAR><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        case GW_MODEL_DP: k_assemble<KIND, true, VT, GW_MODEL_DP><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
+        default: k_assemble<KIND, true, VT><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
     }
 }
 
@@ -361,7 +371,8 @@ template <int KIND>
 int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
                     const double *uo, const gw_bsr_t *A, int prec, double *R, double *force, const PtrsA &a,
                     cudaStream_t s) {
-    const int b = nblk(p.n, kThreads);
+    const int pb = g_tune[GW_TUNE_PARTICLE_BLOCK];
+    const int b = nblk(p.n, pb);
     if (p.n > 0) {
         const int D = KindTraits<KIND>::D, NF = KindTraits<KIND>::NF, NS = KindTraits<KIND>::NS;
         // algorithmic bytes, each array once: particle state in (x, lp, F_old,
@@ -374,15 +385,15 @@ int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const
         const double mat = want_K ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
         ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + grid + mat);
         if (!want_K) {
-            k_assemble<KIND, false, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+            k_assemble<KIND, false, double><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         } else if constexpr (KIND == GW_KIND_SOLID2D) {
             // the 2D solid tangent kernel is instantiated per material, so each
             // carries only its own constitutive code (fewer registers and spills)
             if (prec == GW_PREC_F64) assemble_per_model<KIND, double>(c, p, perm, fm, un, uo, a, R, force, b, s);
             else assemble_per_model<KIND, float>(c, p, perm, fm, un, uo, a, R, force, b, s);
         } else {
-            if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-            else k_assemble<KIND, true, float><<<gw_count_launch(b), kThreads, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+            if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
+            else k_assemble<KIND, true, float><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
         }
         GW_LAUNCHED();
     }
@@ -694,7 +705,8 @@ void mg_carve_hier(Bump &bp, MgHier &h, const gw_grid_t &g0, int64_t n_rows0, in
     gw_grid_t g = g0;
     int64_t nodes = g0.n_nodes;
     int l = 0;
-    for (; l + 1 < kMgMaxLevels && nodes * nf > kMgCoarseMax; ++l) {
+    // levels carved for the smallest coarsest-level bound a caller may set
+    for (; l + 1 < kMgMaxLevels && nodes * nf > kMgCoarseMin; ++l) {
         g = coarse_grid(g);
         nodes = g.n_nodes;
         MgLevel &c = h.lv[l + 1];
@@ -747,7 +759,7 @@ int mg_pattern(MgHier &h, const gw_bsr_t *A0, gw_mg_plan_t *plan, cudaStream_t s
     h.lv[0].L = lat_of(h.lv[0].g);
     h.lv[0].A = *A0;
     int l = 0;
-    while (h.lv[l].A.n_rows * NF > kMgCoarseMax) {
+    while (h.lv[l].A.n_rows * NF > g_tune[GW_TUNE_MG_COARSE]) {
         if (l + 1 >= nl_bound) {
             snprintf(g_msg, sizeof(g_msg), "multigrid: coarsest level still has %d unknowns", h.lv[l].A.n_rows * NF);
             return GW_EINVAL;
@@ -881,13 +893,14 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
                cudaStream_t s) {
     const MgLevel &v = h.lv[l];
     PtrsA a = make_ptrs(v.A);
-    const int g = zero ? red_grid_elems(v.A.n_rows) : red_grid_rows(v.A.n_rows);
+    const int g = zero ? red_grid_elems(v.A.n_rows) : tune_rows_grid(v.A.n_rows);
+    const int tb = zero ? kThreads : tune_rows_block();
     // algorithmic bytes: b, x_out, Minv; with a previous iterate also x_in and the matrix
     const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
     ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
                  2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
-    if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), kThreads, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
-    else k_mg_jacobi<NF, double><<<gw_count_launch(g), kThreads, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
+    if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
+    else k_mg_jacobi<NF, double><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
 }
 
 // One V-cycle on h.lv[0].b; returns the buffer that holds the result (the same
@@ -908,10 +921,10 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
             const double mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
             ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
             if (l == 0)
-                k_mg_presmooth2<NF, VT><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(
+                k_mg_presmooth2<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
                     a, v.Minv, v.b, y, kMgOmega, skip);
             else
-                k_mg_presmooth2<NF, double><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(
+                k_mg_presmooth2<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
                     a, v.Minv, v.b, y, kMgOmega, skip);
             double *t = x; x = y; y = t;
         } else {
@@ -925,8 +938,8 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         const double vs = 8.0 * v.A.n_rows * NF;
         {
         ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4));
-        if (l == 0) k_mg_residual<NF, VT><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(a, v.b, x, v.r, skip);
-        else k_mg_residual<NF, double><<<gw_count_launch(red_grid_rows(v.A.n_rows)), kThreads, 0, s>>>(a, v.b, x, v.r, skip);
+        if (l == 0) k_mg_residual<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
+        else k_mg_residual<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
         }
         ProfScope ps(PC_MG_TRANSFER, s, vs + 8.0 * c.A.n_rows * NF);
         if (D == 2) k_mg_restrict<2, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, v.r, c.b, skip);
@@ -962,7 +975,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
 // instantiated graph serves all Newton iterations of a load step.  The graphs
 // are held in a small cache (least recently used entry replaced).
 struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, pad;
+    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps;
     int n_grid[3];
     int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
     gw_bsr_t A;
@@ -1011,6 +1024,7 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
     memset(&k, 0, sizeof(k));
     GW_CUDA(cudaGetDevice(&k.device));
     k.nf = NF; k.vt_bytes = sizeof(VT); k.restart = restart; k.nl = h.nl; k.dn = h.dn; k.dim = grid.dim;
+    k.row_warps = g_tune[GW_TUNE_ROW_WARPS];
     for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
     for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
     k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;
@@ -1449,7 +1463,8 @@ extern "C" int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, c
     LaunchConst c = make_lc(grid, mat, st);
     c.mc.tip_tangent = 0.0;  // exact derivatives of the converged state
     ProfScope ps(PC_ADJ_G2P, s, (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 18 + 23 + 2 * 9 * 2));
-    const dim3 grd(gw_count_launch(nblk(pt->n, 128))), blk(128);
+    const int ab = g_tune[GW_TUNE_ADJOINT_BLOCK];
+    const dim3 grd(gw_count_launch(nblk(pt->n, ab))), blk(ab);
     const PtrsP pp = make_ptrs(*pt);
     const PtrsA pa = make_ptrs(*A);
     const AdjState si = make_adj(*seed_in), qo = make_adj(*q_out);
@@ -1476,7 +1491,8 @@ extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *m
     LaunchConst c = make_lc(grid, mat, st);
     c.mc.tip_tangent = 0.0;  // exact derivatives of the converged residual
     ProfScope ps(PC_ADJ_RES, S(stream), (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 23 * 2 + 2 * 9 * 2 + 9 * 2));
-    const dim3 grd(gw_count_launch(nblk(pt->n, 128))), blk(128);
+    const int ab = g_tune[GW_TUNE_ADJOINT_BLOCK];
+    const dim3 grd(gw_count_launch(nblk(pt->n, ab))), blk(ab);
     const PtrsP pp = make_ptrs(*pt);
     const PtrsA pa = make_ptrs(*A);
     const AdjState qo = make_adj(*q_out);
@@ -1495,6 +1511,27 @@ extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *m
 
 // ==================================================================== kernel timing
 extern "C" int64_t gw_launch_count(void) { return g_launches; }
+
+extern "C" int gw_tune_set(int32_t knob, int32_t value) {
+    switch (knob) {
+        case GW_TUNE_PARTICLE_BLOCK:
+        case GW_TUNE_ADJOINT_BLOCK:  // the particle kernels use up to 255 registers: 256 threads at most
+            if (value < 32 || value > 256 || value % 32) return GW_EINVAL;
+            break;
+        case GW_TUNE_ROW_WARPS:
+            if (value < 1 || value > 32) return GW_EINVAL;
+            break;
+        case GW_TUNE_MG_COARSE:
+            if (value < kMgCoarseMin || value > kMgCoarseMax) return GW_EINVAL;
+            break;
+        default:
+            return GW_EINVAL;
+    }
+    g_tune[knob] = value;
+    return GW_OK;
+}
+
+extern "C" int32_t gw_tune_get(int32_t knob) { return (knob >= 0 && knob < GW_TUNE_COUNT) ? g_tune[knob] : -1; }
 
 extern "C" int gw_profile_enable(int32_t on) {
     g_prof_on = on != 0;

@@ -37,6 +37,7 @@ constexpr int kMgMaxLevels = GW_MG_MAX_LEVELS;
 // unknowns of the coarsest (dense) level: its n x n FP64 matrix (204,800 bytes
 // at 160) is inverted in one CTA's shared memory
 constexpr int kMgCoarseMax = 160;
+constexpr int kMgCoarseMin = 8;  // smallest coarsest-level bound a caller may set
 
 // lattice node counts of a grid (cells + 1 per axis; 1 on unused axes)
 struct Lat {

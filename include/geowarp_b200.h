@@ -384,6 +384,31 @@ int64_t gw_launch_count(void);
 int gw_profile_read(int32_t cls, double *ms_total_host, int64_t *launches_host, double *bytes_host);
 const char *gw_profile_name(int32_t cls);
 
+/* ------------------------------------------------------------ launch-shape knobs
+ * Process-wide settings the autotuner (geowarp_b200/autotune.py) searches per
+ * workload on the device it runs on; no counterpart in the reference, whose
+ * kernels Warp launches with fixed shapes.  They take effect at the next
+ * launch (a changed GW_TUNE_ROW_WARPS recaptures the multigrid step graphs; a
+ * changed GW_TUNE_MG_COARSE applies to plans built afterwards).
+ *   GW_TUNE_PARTICLE_BLOCK  threads per CTA of the residual/tangent assembly,
+ *                           32..256, a multiple of 32 (default 256)
+ *   GW_TUNE_ADJOINT_BLOCK   threads per CTA of the adjoint particle kernels,
+ *                           32..256, a multiple of 32 (default 128)
+ *   GW_TUNE_ROW_WARPS       warps per CTA of the multigrid smoothing and
+ *                           residual kernels (one warp per block row), 1..32
+ *                           (default 8)
+ *   GW_TUNE_MG_COARSE       most unknowns of the dense coarsest multigrid
+ *                           level, 8..160 (default 160)
+ * gw_tune_set returns GW_EINVAL outside these ranges; gw_tune_get returns -1
+ * for an unknown knob. */
+#define GW_TUNE_PARTICLE_BLOCK 0
+#define GW_TUNE_ADJOINT_BLOCK 1
+#define GW_TUNE_ROW_WARPS 2
+#define GW_TUNE_MG_COARSE 3
+#define GW_TUNE_COUNT 4
+int gw_tune_set(int32_t knob, int32_t value);
+int32_t gw_tune_get(int32_t knob);
+
 #ifdef __cplusplus
 }
 #endif

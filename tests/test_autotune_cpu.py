@@ -1,0 +1,50 @@
+"""Launch-shape knobs and the autotuner's search, on the host: gw_tune_set /
+gw_tune_get only touch host state, so the library answers them without a
+GPU, and the search is driven by a synthetic cost with a known optimum."""
+import pytest
+
+from geowarp_b200 import _lib as L
+from geowarp_b200 import autotune
+
+DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160}
+
+
+@pytest.fixture
+def lib():
+    lib = L.load()
+    yield lib
+    for k, v in DEFAULTS.items():
+        assert lib.gw_tune_set(k, v) == L.GW_OK
+
+
+def test_knob_defaults_and_ranges(lib):
+    for k, v in DEFAULTS.items():
+        assert lib.gw_tune_get(k) == v
+    assert lib.gw_tune_get(L.TUNE_COUNT) == -1
+    bad = [(L.TUNE_PARTICLE_BLOCK, 288), (L.TUNE_PARTICLE_BLOCK, 48), (L.TUNE_ADJOINT_BLOCK, 0),
+           (L.TUNE_ROW_WARPS, 0), (L.TUNE_ROW_WARPS, 33), (L.TUNE_MG_COARSE, 7), (L.TUNE_MG_COARSE, 161),
+           (L.TUNE_COUNT, 1)]
+    for k, v in bad:
+        assert lib.gw_tune_set(k, v) == L.GW_EINVAL, (k, v)
+        if k != L.TUNE_COUNT:
+            assert lib.gw_tune_get(k) == DEFAULTS[k]  # a rejected value leaves the knob alone
+    for k, v in [(L.TUNE_PARTICLE_BLOCK, 64), (L.TUNE_ADJOINT_BLOCK, 256), (L.TUNE_ROW_WARPS, 2),
+                 (L.TUNE_MG_COARSE, 40)]:
+        assert lib.gw_tune_set(k, v) == L.GW_OK
+        assert lib.gw_tune_get(k) == v
+
+
+def test_coordinate_search_finds_the_separable_optimum(lib):
+    target = {"row_warps": 4, "mg_coarse": 80, "particle_block": 128, "adjoint_block": 64}
+
+    def cost():
+        cfg = autotune.current()
+        return sum((cfg[n] - target[n]) ** 2 / float(target[n]) for n in target) + 1.0
+
+    calls = []
+    best, table = autotune.tune(lambda: calls.append(1), reps=3, timer=lambda fn: (fn(), cost())[1])
+    assert best == target
+    assert autotune.current() == target          # the winners stay set
+    assert set(table) == set(autotune.KNOBS)
+    n_cands = sum(len(c) for _, c in autotune.KNOBS.values())
+    assert len(calls) == n_cands * 4             # one untimed + three timed trials per candidate

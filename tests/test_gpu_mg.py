@@ -164,3 +164,35 @@ def test_mg_workspace_too_small_is_rejected(cuda):
                                    30, _p(ws), ws.numel(), C.byref(it), C.byref(rr), e.stream)
     assert rc == L.GW_EINVAL
     assert b"workspace" in lib.gw_status_string(rc)
+
+
+def test_launch_knobs_change_speed_not_results(cuda):
+    """The autotuner's knobs (CTA sizes, the dense coarsest level bound) leave
+    the converged load steps as they are: same forward state and gradient as
+    with the default knobs, to the Krylov tolerance."""
+    from geowarp_b200 import _lib as L
+    from geowarp_b200 import problems
+    from geowarp_b200.adjoint import LoadStepAdjoint
+    lib = L.load()
+    defaults = {k: lib.gw_tune_get(k) for k in range(L.TUNE_COUNT)}
+
+    def run():
+        s = problems.bar_compaction_2d(precision="fp64", device=cuda)
+        adj = LoadStepAdjoint(s)
+        for k in range(3):
+            adj.forward_step(k, 50, keep=False)
+            adj.seed_displacement_misfit()
+            adj.backward_step()
+        return (s.x_particles - s.x0).cpu().numpy(), adj.grad_E.cpu().numpy()
+
+    try:
+        u0, g0 = run()
+        for k, v in [(L.TUNE_PARTICLE_BLOCK, 64), (L.TUNE_ADJOINT_BLOCK, 64), (L.TUNE_ROW_WARPS, 2),
+                     (L.TUNE_MG_COARSE, 40)]:
+            assert lib.gw_tune_set(k, v) == L.GW_OK
+        u1, g1 = run()
+    finally:
+        for k, v in defaults.items():
+            lib.gw_tune_set(k, v)
+    assert rel_err(u1, u0) < 1e-9
+    assert rel_err(g1, g0) < 1e-7
