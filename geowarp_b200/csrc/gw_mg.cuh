@@ -500,75 +500,78 @@ __global__ void k_mg_dense_build(PtrsA A, double *__restrict__ M, int n) {
 // lowest row: the result is deterministic.
 __global__ void k_mg_dense_invert(const double *__restrict__ M, double *__restrict__ Inv, int n) {
     extern __shared__ double a[];
-    __shared__ int perm[kMgCoarseMax];
-    __shared__ double fk[kMgCoarseMax];
-    __shared__ int piv_s;
-    __shared__ double red_v[32];
-    __shared__ int red_i[32];
+    __shared__ int perm[kMgCoarseMax], colsrc[kMgCoarseMax];
+    __shared__ double fk[kMgCoarseMax], prow[kMgCoarseMax], oldk[kMgCoarseMax];
+    __shared__ int piv_s, unit_s;
     const int t = threadIdx.x, nt = blockDim.x, lane = t & 31, w = t >> 5;
     for (int q = t; q < n * n; q += nt) a[q] = M[q];
     __syncthreads();
+    // elimination threads: column j, row group g of G (each keeps its pivot-row
+    // entry in a register; the multipliers fk[i] are broadcast reads)
+    const int G = nt / n, j = t % n, g = t / n;
     for (int k = 0; k < n; ++k) {
-        double best = -1.0;
-        int bi = k;
-        for (int i = k + t; i < n; i += nt) {
-            const double v = fabs(a[i * n + k]);
-            if (v > best) { best = v; bi = i; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_down_sync(0xffffffffu, best, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
-        }
-        if (lane == 0) { red_v[w] = best; red_i[w] = bi; }
-        __syncthreads();
-        if (t == 0) {
-            double bv = red_v[0];
-            int b = red_i[0];
-            for (int q = 1; q < (nt >> 5); ++q)
-                if (red_v[q] > bv || (red_v[q] == bv && red_i[q] < b)) { bv = red_v[q]; b = red_i[q]; }
-            if (!(bv > 0.0)) {  // no nonzero pivot: unit pivot in place
-                a[k * n + k] = 1.0;
-                b = k;
+        // 1. pivot: the first row of largest |a_ik|, i >= k (warp 0)
+        if (w == 0) {
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + lane; i < n; i += 32) {
+                const double v = fabs(a[i * n + k]);
+                if (v > best) { best = v; bi = i; }
             }
-            piv_s = b;
-            perm[k] = b;
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (lane == 0) {
+                const int unit = !(best > 0.0);  // no nonzero pivot: unit pivot in place
+                piv_s = unit ? k : bi;
+                unit_s = unit;
+                perm[k] = piv_s;
+            }
         }
         __syncthreads();
-        const int p = piv_s;
-        if (p != k)
-            for (int j = t; j < n; j += nt) {
-                const double tmp = a[k * n + j];
-                a[k * n + j] = a[p * n + j];
-                a[p * n + j] = tmp;
+        // 2. stage the swapped-in pivot row scaled by 1/pivot, the old row k
+        //    (it moves to row p) and column k of the row-swapped matrix
+        const int p = piv_s, unit = unit_s;
+        const double pinv = 1.0 / (unit ? 1.0 : a[p * n + k]);
+        if (t < n) {
+            const double rp = (unit && t == k) ? 1.0 : a[p * n + t];
+            prow[t] = (t == k) ? pinv : rp * pinv;
+            oldk[t] = a[k * n + t];
+        } else if (t < 2 * n) {
+            const int i = t - n;
+            const int src = (i == k) ? p : (i == p ? k : i);
+            fk[i] = (unit && i == k) ? 1.0 : a[src * n + k];
+        }
+        __syncthreads();
+        // 3. row k := pivot row; every other row i: a_ij -= fk_i prow_j, a_ik := -fk_i / pivot
+        if (g < G) {
+            const double pj = prow[j], ok = oldk[j];
+            for (int i = g; i < n; i += G) {
+                if (i == k) { a[k * n + j] = pj; continue; }
+                const double f = fk[i];
+                const double v = (i == p) ? ok : a[i * n + j];
+                if (j == k) a[i * n + j] = -f * pinv;
+                else a[i * n + j] = (f != 0.0) ? v - f * pj : v;
             }
-        __syncthreads();
-        const double pinv = 1.0 / a[k * n + k];
-        for (int i = t; i < n; i += nt) fk[i] = a[i * n + k];
-        __syncthreads();
-        for (int j = t; j < n; j += nt) a[k * n + j] = (j == k) ? pinv : a[k * n + j] * pinv;
-        __syncthreads();
-        for (int q = t; q < n * n; q += nt) {
-            const int i = q / n, j = q - (q / n) * n;
-            if (i == k) continue;
-            const double f = fk[i];
-            if (j == k) a[q] = -f * pinv;
-            else if (f != 0.0) a[q] -= f * a[k * n + j];
         }
         __syncthreads();
     }
-    // undo the row interchanges as column interchanges, last first
-    for (int k = n - 1; k >= 0; --k) {
-        const int p = perm[k];
-        if (p != k)
-            for (int i = t; i < n; i += nt) {
-                const double tmp = a[i * n + k];
-                a[i * n + k] = a[i * n + p];
-                a[i * n + p] = tmp;
-            }
-        __syncthreads();
+    // undo the row interchanges as column interchanges, last first: compose
+    // them into one column map and apply it while writing out
+    if (t == 0) {
+        for (int q = 0; q < n; ++q) colsrc[q] = q;
+        for (int k = n - 1; k >= 0; --k) {
+            const int p = perm[k];
+            const int tmp = colsrc[k]; colsrc[k] = colsrc[p]; colsrc[p] = tmp;
+        }
     }
-    for (int q = t; q < n * n; q += nt) Inv[q] = a[q];
+    __syncthreads();
+    for (int q = t; q < n * n; q += nt) {
+        const int i = q / n, c = q - i * n;
+        Inv[q] = a[i * n + colsrc[c]];
+    }
 }
 
 // x = Inv b (one warp per row)
