@@ -1395,8 +1395,11 @@ extern "C" int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_parti
     LaunchConst c = make_lc(grid, nullptr, st);
     PtrsP p = make_ptrs(*pt);
     const int b = nblk(pt->n, kThreads);
-    ProfScope ps(PC_G2P, S(stream), (double)pt->n * 8.0 * (2 * grid->dim * 3 + 9 * 4 + 3) +
-                                        (double)pt->n * 27.0 * 8.0 * grid->nf * 2);
+    // algorithmic bytes, each array once: per particle x and lp in and out,
+    // F_new and b_new in, F_old and b_old out, pi and the pore pressure; the
+    // two nodal solution vectors once per node
+    ProfScope ps(PC_G2P, S(stream), (double)pt->n * 8.0 * (4 * grid->dim + 9 * 4 + 3) +
+                                        2.0 * 8.0 * grid->nf * (double)grid->n_nodes);
     switch (grid->kind) {
         case GW_KIND_SOLID2D: k_g2p<GW_KIND_SOLID2D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;
         case GW_KIND_COUPLED2D: k_g2p<GW_KIND_COUPLED2D><<<gw_count_launch(b), kThreads, 0, S(stream)>>>(c, p, u_new, u_old); break;

@@ -35,4 +35,15 @@ def roofline_summary(rec, peaks, peak_kind="measured"):
             "traffic": None, "launches": v["launches"], "avg_launch_us": avg_ms * 1e3,
             "bytes_per_launch": bytes_per_launch,
             "share_of_instrumented_time": v["ms"] / tot,
-            "breakdown_ms": {k: round(x["ms"], 3) for k, x in rec.items()}}
+            "breakdown_ms": {k: round(x["ms"], 3) for k, x in rec.items()},
+            "per_class": {k: _class_entry(x, peak) for k, x in rec.items() if x["launches"] > 0}}
+
+
+def _class_entry(v, peak):
+    """Average launch of one timing class: achieved algorithmic GB/s and its
+    fraction of the HBM peak."""
+    avg_ms = v["ms"] / max(v["launches"], 1)
+    bpl = v["bytes"] / max(v["launches"], 1)
+    gbs = bpl / (avg_ms * 1e-3) / 1e9 if avg_ms > 0 else 0.0
+    return {"launches": v["launches"], "avg_launch_us": round(avg_ms * 1e3, 3), "bytes_per_launch": round(bpl),
+            "achieved_gbs": round(gbs, 1), "frac": round(gbs / peak, 4)}
