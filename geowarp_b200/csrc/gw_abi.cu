@@ -84,6 +84,14 @@ inline int gw_count_launch(int grid) {
     return grid;
 }
 inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
+// The row kernels gather 2x2 and 4x4 blocks and their vectors with 16-byte
+// loads: those systems need 16-byte aligned values and vectors.
+inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
+inline bool vec_ok(const gw_bsr_t *A, const void *u, const void *v) {
+    if (A->nf != 2 && A->nf != 4) return true;
+    return aligned16(A->vals) && aligned16(u) && aligned16(v);
+}
+
 // launch-shape knobs (gw_tune_set): particle CTA, adjoint CTA, warps per CTA
 // of the multigrid row kernels, bound of the dense coarsest level
 int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160};
@@ -617,6 +625,7 @@ extern "C" int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t preco
                                   double rtol, int32_t max_iter, int32_t restart, void *workspace, int32_t *iters_host,
                                   double *relres_host, void *stream) {
     GW_REQUIRE(A && b && x && workspace && iters_host && relres_host && max_iter > 0);
+    GW_REQUIRE(vec_ok(A, b, x));
     GW_REQUIRE(restart >= 1 && restart <= kGmresMaxRestart);
     int it = 0;
     double rr = 0.0;
@@ -1232,6 +1241,7 @@ extern "C" int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, i
                                      int32_t max_iter, int32_t restart, void *workspace, int64_t workspace_bytes,
                                      int32_t *iters_host, double *relres_host, void *stream) {
     GW_REQUIRE(grid && A && b && x && workspace && iters_host && relres_host && max_iter > 0);
+    GW_REQUIRE(vec_ok(A, b, x));
     GW_REQUIRE(restart >= 1 && restart <= kGmresMaxRestart);
     int rc = mg_check_args(grid, A);
     if (rc) return rc;
@@ -1256,6 +1266,7 @@ extern "C" int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t meth
                                    double *x, double rtol, int32_t max_iter, void *workspace, int32_t *iters_host,
                                    double *relres_host, void *stream) {
     GW_REQUIRE(A && b && x && workspace && iters_host && relres_host && max_iter > 0);
+    GW_REQUIRE(vec_ok(A, b, x));
     int it = 0;
     double rr = 0.0;
     int rc = (prec == GW_PREC_F64)
@@ -1312,6 +1323,7 @@ extern "C" int gw_bsr_krylov_solve_static(const gw_bsr_t *A, int32_t prec, int32
                                           const double *b, double *x, double rtol, int32_t max_iter,
                                           int32_t *iters_host, double *relres_host, void *stream) {
     GW_REQUIRE(A && b && x && iters_host && relres_host && max_iter > 0);
+    GW_REQUIRE(vec_ok(A, b, x));
     const int64_t unknowns = (int64_t)A->n_rows * A->nf;
     if (A->n_rows < 0 || A->nf < 1 || A->nf > 4 || unknowns > kStaticKrylovMaxUnknowns ||
         krylov_ws_bytes(A->n_rows, A->nf) > kStaticKrylovBytes) {
@@ -1361,6 +1373,7 @@ int spmv_any(const gw_bsr_t *A, const double *x, double *y, bool trans, cudaStre
 
 extern "C" int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream) {
     GW_REQUIRE(A && x && y);
+    GW_REQUIRE(vec_ok(A, x, y));
     return prec == GW_PREC_F64 ? spmv_any<double>(A, x, y, false, S(stream)) : spmv_any<float>(A, x, y, false, S(stream));
 }
 

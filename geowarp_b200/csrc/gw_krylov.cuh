@@ -78,6 +78,55 @@ __device__ __forceinline__ bool grid_reduce(double v[NV], double *partials, unsi
 }
 
 // ---------------------------------------------------------------- SpMV
+// Vectorised gathers of one NF x NF block and one NF-vector: 16-byte loads
+// for NF = 2 and 4 (block values and vectors 16-byte aligned; the entry
+// points check it), scalar loads otherwise.  The values and the order they
+// are used in are the same either way.
+template <int NF, typename VT>
+__device__ __forceinline__ void load_block(const VT *__restrict__ p, double out[NF * NF]) {
+#pragma unroll
+    for (int i = 0; i < NF * NF; ++i) out[i] = (double)p[i];
+}
+template <>
+__device__ __forceinline__ void load_block<2, float>(const float *__restrict__ p, double out[4]) {
+    const float4 v = *reinterpret_cast<const float4 *>(p);
+    out[0] = v.x; out[1] = v.y; out[2] = v.z; out[3] = v.w;
+}
+template <>
+__device__ __forceinline__ void load_block<2, double>(const double *__restrict__ p, double out[4]) {
+    const double2 a = reinterpret_cast<const double2 *>(p)[0], b = reinterpret_cast<const double2 *>(p)[1];
+    out[0] = a.x; out[1] = a.y; out[2] = b.x; out[3] = b.y;
+}
+template <>
+__device__ __forceinline__ void load_block<4, float>(const float *__restrict__ p, double out[16]) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 v = reinterpret_cast<const float4 *>(p)[q];
+        out[4 * q] = v.x; out[4 * q + 1] = v.y; out[4 * q + 2] = v.z; out[4 * q + 3] = v.w;
+    }
+}
+template <>
+__device__ __forceinline__ void load_block<4, double>(const double *__restrict__ p, double out[16]) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const double2 v = reinterpret_cast<const double2 *>(p)[q];
+        out[2 * q] = v.x; out[2 * q + 1] = v.y;
+    }
+}
+template <int NF>
+__device__ __forceinline__ void load_vec(const double *__restrict__ p, double out[NF]) {
+    if constexpr (NF == 2 || NF == 4) {
+#pragma unroll
+        for (int q = 0; q < NF / 2; ++q) {
+            const double2 v = reinterpret_cast<const double2 *>(p)[q];
+            out[2 * q] = v.x; out[2 * q + 1] = v.y;
+        }
+    } else {
+#pragma unroll
+        for (int g = 0; g < NF; ++g) out[g] = p[g];
+    }
+}
+
 // One warp per block row; lanes stride over the row's blocks.
 template <int NF, typename VT>
 __device__ __forceinline__ void row_mv(const PtrsA &A, int r, const double *__restrict__ x, double acc[NF]) {
@@ -88,14 +137,13 @@ __device__ __forceinline__ void row_mv(const PtrsA &A, int r, const double *__re
     const VT *vals = (const VT *)A.vals;
     for (int j = s + lane; j < e; j += 32) {
         const int col = A.cols[j];
-        double xv[NF];
-#pragma unroll
-        for (int g = 0; g < NF; ++g) xv[g] = x[(size_t)col * NF + g];
-        const VT *blk = vals + (size_t)j * NF * NF;
+        double xv[NF], bv[NF * NF];
+        load_vec<NF>(x + (size_t)col * NF, xv);
+        load_block<NF, VT>(vals + (size_t)j * NF * NF, bv);
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
-            for (int g = 0; g < NF; ++g) acc[f] += (double)blk[f * NF + g] * xv[g];
+            for (int g = 0; g < NF; ++g) acc[f] += bv[f * NF + g] * xv[g];
     }
 #pragma unroll
     for (int f = 0; f < NF; ++f)

@@ -363,15 +363,14 @@ __global__ void k_mg_presmooth2(PtrsA A, const double *__restrict__ Minv, const 
         const int s0 = A.row_ptr[r], e0 = A.row_ptr[r + 1];
         for (int j = s0 + lane; j < e0; j += 32) {
             const int col = A.cols[j];
-            double t[NF], z[NF];
-#pragma unroll
-            for (int g = 0; g < NF; ++g) t[g] = b[(size_t)col * NF + g];
+            double t[NF], z[NF], bv[NF * NF];
+            load_vec<NF>(b + (size_t)col * NF, t);
+            load_block<NF, VT>(vals + (size_t)j * NF * NF, bv);
             apply_minv<NF>(Minv, col, t, z);
-            const VT *blk = vals + (size_t)j * NF * NF;
 #pragma unroll
             for (int f = 0; f < NF; ++f)
 #pragma unroll
-                for (int g = 0; g < NF; ++g) acc[f] += (double)blk[f * NF + g] * (omega * z[g]);
+                for (int g = 0; g < NF; ++g) acc[f] += bv[f * NF + g] * (omega * z[g]);
         }
 #pragma unroll
         for (int f = 0; f < NF; ++f)

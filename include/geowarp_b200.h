@@ -134,7 +134,10 @@ typedef struct gw_particles {
 } gw_particles_t;
 
 /* Block-CSR over active nodes.  Block (r, j) is nf x nf, row-major, at
- * vals[(row_ptr[r] + j)*nf*nf].  cols[] are active-row indices. */
+ * vals[(row_ptr[r] + j)*nf*nf].  cols[] are active-row indices.  With nf = 2
+ * or 4 the SpMV and Krylov entry points gather blocks and vectors with
+ * 16-byte loads: vals and the FP64 vectors passed to them must be 16-byte
+ * aligned (GW_EINVAL otherwise). */
 typedef struct gw_bsr {
     int32_t n_rows;
     int32_t nf;

@@ -96,3 +96,22 @@ def test_unknown_material_raises():
     from geowarp_b200.engine import material_struct
     with pytest.raises(ValueError):
         material_struct(dict(material_name="Mohr-Coulomb"))
+
+
+def test_vectorised_entry_points_reject_misaligned_vectors():
+    """2x2 / 4x4 systems are gathered with 16-byte loads: a vector that is not
+    16-byte aligned is rejected on the host, before any launch or access."""
+    import ctypes as C
+    import numpy as np
+    from geowarp_b200 import _lib as L
+    lib = L.load()
+    buf = np.zeros(64, dtype=np.float64)
+    base = buf.ctypes.data
+    off = base + (16 - base % 16) % 16          # 16-byte aligned address inside buf
+    A = L.Bsr()
+    A.n_rows, A.nf, A.nnzb, A.mask_words = 2, 2, 2, 1
+    p = C.c_void_p(off)
+    A.row_ptr = A.cols = A.row2node = A.node2row = A.stencil = A.vals = p
+    rc = lib.gw_bsr_spmv(C.byref(A), L.PREC_F64, C.c_void_p(off + 8), p, None)
+    assert rc == L.GW_EINVAL
+    assert b"vec_ok" in lib.gw_status_string(rc)
