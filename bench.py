@@ -17,6 +17,10 @@ collective) and `value` is the aggregate over ranks.
 load steps with their own time increments; the adjoint covers the 2D solid
 solver); --workload bar runs the 4 x 40-cell self-weight bar.
 
+Before the timed region, --autotune on (the default) searches the library's
+launch-shape knobs on the workload's own load step (geowarp_b200.autotune); the
+chosen values apply to every arm and are reported in the line.
+
 --impl reference times the CPU restatement of the reference's algorithm (the
 reference itself runs only on NVIDIA Warp, not installable here) on a bounded
 sample of the same workload.
