@@ -1000,6 +1000,7 @@ struct MgGraphEntry {
     uint64_t stamp;
 };
 constexpr int kMgGraphCache = 8;
+int g_gm_last_iters = 0;  // iterations of the previous multigrid GMRES solve (first-chunk hint)
 MgGraphEntry g_mg_graphs[kMgGraphCache];
 uint64_t g_mg_graph_clock = 0;
 cudaStream_t g_capture_stream[64] = {};
@@ -1140,7 +1141,12 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
         GW_CUDA(cudaMemcpyAsync(&hs, G.sc, head, cudaMemcpyDeviceToHost, s));
         GW_CUDA(cudaStreamSynchronize(s));
         if (hs.done) break;
-        int chunk = 4;
+        // Arnoldi steps queued before the next host check: the previous
+        // solve's iteration count to start with (Newton solves of a step look
+        // alike), then the iterations left at the observed convergence rate.
+        // Steps queued past convergence still launch their (early-exiting)
+        // kernels, so the estimate trims them without adding host reads.
+        int chunk = g_gm_last_iters > 0 ? std::min(std::max(g_gm_last_iters, 2), 16) : 4;
         int kk = 0;
         const double spmv_bytes = (double)A->nnzb * (NF * NF * sizeof(VT) + 4) + 4.0 * (nr + 1) + 24.0 * n;
         cudaGraphExec_t step_graph = nullptr;
@@ -1170,7 +1176,15 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
             GW_CUDA(cudaMemcpyAsync(&hs, G.sc, head, cudaMemcpyDeviceToHost, s));
             GW_CUDA(cudaStreamSynchronize(s));
             if (hs.cycle_done) break;
-            chunk = chunk < 16 ? chunk * 2 : 16;
+            int next = chunk < 16 ? chunk * 2 : 16;
+            if (hs.k > 0 && hs.beta > 0.0 && hs.resid > 0.0 && hs.resid < hs.beta && hs.tol > 0.0) {
+                const double rate = ::pow(hs.resid / hs.beta, 1.0 / hs.k);
+                if (rate < 1.0) {
+                    const double left = ::ceil(::log(hs.tol / hs.resid) / ::log(rate));
+                    next = left < 1.0 ? 1 : (left > 16.0 ? 16 : (int)left);
+                }
+            }
+            chunk = next;
         }
         if (hs.status) break;
         k_gm_solve_y<<<gw_count_launch(1), 32, 0, s>>>(G.sc);
@@ -1179,6 +1193,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
     }
     *iters = hs.iters;
     *relres = (hs.bnorm > 0.0) ? hs.resid / hs.bnorm : 0.0;
+    g_gm_last_iters = hs.iters;
     if (hs.status == ST_NAN) return GW_ENAN;
     if (hs.resid > hs.tol) return GW_ENOCONV;
     return GW_OK;
