@@ -530,68 +530,71 @@ def roofline_pass(adj, k, wl):
     return profiling.roofline_summary(kt, peaks, peak_kind="measured" if "when" in peaks else "fallback")
 
 
-def cpu_baseline(wl, gpu_line):
-    """Oracle (CPU restatement) timing on a bounded sample, run on rank 0: one
-    load step of the 64x32-cell footing variant, scaled to the workload's
-    particle count."""
+def host_threads():
+    """Host cores this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def oracle_rate(wl, steps=2, budget_s=15.0):
+    """The oracle (CPU restatement of the reference's algorithm) on a bounded
+    sample of the workload, with every host core on the tangent's
+    complex-step passes: (load steps per second in the workload's unit,
+    threads, description)."""
+    # the tangent of a 2D step is 9 nodes x nf complex-step passes: more
+    # threads than passes would sit idle, and are not counted
+    nf = 3 if isinstance(wl, ConsolidationWorkload) else 2
+    th = max(1, min(host_threads(), 9 * nf))
     if isinstance(wl, ConsolidationWorkload):
         from oracle.bench_sample import oracle_consolidation_sample
-        sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts)
-        return {"value": 1.0 / sec, "unit": gpu_line["unit"], "cores": 1, "kind": "port", "sample": sample}
+        sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts, max_steps=max(steps, 3),
+                                                     budget_s=budget_s, threads=th)
+        return 1.0 / sec, th, sample
     if isinstance(wl, BarWorkload):
         from oracle.bench_sample import oracle_bar_sample
-        sec, n, sample = oracle_bar_sample(wl.n_steps)
-        return {"value": 1.0 / sec, "unit": gpu_line["unit"], "cores": 1, "kind": "port",
-                "sample": sample + " (forward load steps; the CPU path has no adjoint)"}
+        sec, n, sample = oracle_bar_sample(wl.n_steps, max_steps=max(steps, 3), budget_s=budget_s, threads=th)
+        return 1.0 / sec, th, sample + " (forward load steps; the CPU path has no adjoint)"
     from oracle.bench_sample import oracle_load_step_sample
-    sec, its, sample = oracle_load_step_sample()
+    times = []
+    for k in range(max(1, min(steps, 2))):
+        sec, its, sample = oracle_load_step_sample(step=k, threads=th)
+        times.append(sec)
     scale = 1.0
     if isinstance(wl, BatchedWorkload):
         # per-particle work dominates the oracle step: scale by particles
         scale = wl.config["particles"] / 131072.0
         sample += f"; scaled to the batch by x{scale:.2f} (particles)"
-    return {"value": wl.units / (sec * scale), "unit": gpu_line["unit"], "cores": 1, "kind": "port",
-            "sample": sample + " (forward load step; the CPU path has no adjoint)"}
+    return wl.units / (float(np.mean(times)) * scale), th, sample + " (forward load step; the CPU path has no adjoint)"
+
+
+def cpu_baseline(wl, gpu_line):
+    """Oracle timing on a bounded sample, run on rank 0 (one load step of the
+    64x32-cell footing variant scaled to the workload, or the first load steps
+    of the bar / column)."""
+    v, th, sample = oracle_rate(wl, steps=1)
+    return {"value": v, "unit": gpu_line["unit"], "cores": th, "kind": "port", "sample": sample}
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(args):
     """The reference's algorithm on the host cores: the CPU restatement (the
-    reference itself needs NVIDIA Warp, which is not installable here), one
-    complete load step of the 64x32-cell variant per step, scaled to the
-    full workload.  Rank 0 only."""
+    reference itself needs NVIDIA Warp, which is not installable here) with
+    every host core on its tangent passes, on a bounded sample of the
+    workload.  Rank 0 only."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     wl = make_workload(args)
-    if isinstance(wl, ConsolidationWorkload):
-        from oracle.bench_sample import oracle_consolidation_sample
-        sec, n, sample = oracle_consolidation_sample(wl.dicts[:6], wl.dts, max_steps=max(args.steps, 3),
-                                                     budget_s=60.0)
-        v = 1.0 / sec
-    elif isinstance(wl, BarWorkload):
-        from oracle.bench_sample import oracle_bar_sample
-        sec, n, sample = oracle_bar_sample(wl.n_steps, max_steps=max(args.steps, 3), budget_s=60.0)
-        sample += " (forward load steps; the CPU path has no adjoint)"
-        v = 1.0 / sec
-    else:
-        from oracle.bench_sample import oracle_load_step_sample
-        times = []
-        for k in range(max(1, min(args.steps, 2))):
-            sec, its, sample = oracle_load_step_sample(step=k)
-            times.append(sec)
-        scale = wl.config["particles"] / 131072.0 if isinstance(wl, BatchedWorkload) else 1.0
-        if scale != 1.0:
-            sample += f"; scaled to the batch by x{scale:.2f} (particles)"
-        sample += " (forward load step; the CPU path has no adjoint)"
-        v = wl.units / (float(np.mean(times)) * scale)
+    v, th, sample = oracle_rate(wl, steps=args.steps, budget_s=60.0)
     unit = wl.metric.split(" (")[0]
     print(json.dumps({
         "impl": "reference", "metric": wl.metric, "value": v, "unit": unit, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-        "dtype": "f64", "data": "synthetic", "config": dict(wl.config, parallelism="host cores x1"),
-        "cpu_baseline": {"value": v, "unit": unit, "cores": 1, "kind": "port", "sample": sample},
+        "dtype": "f64", "data": "synthetic", "config": dict(wl.config, parallelism=f"host cores x{th}"),
+        "cpu_baseline": {"value": v, "unit": unit, "cores": th, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 

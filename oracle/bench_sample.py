@@ -88,16 +88,18 @@ def oracle_newton_sample(footing_kwargs=None, full=(256, 128)):
     return est, desc
 
 
-def oracle_load_step_sample(footing_kwargs=None, full=(256, 128), step=0):
+def oracle_load_step_sample(footing_kwargs=None, full=(256, 128), step=0, threads=1):
     """Seconds per load step of the full-size footing, from one complete load
     step (P2G, Newton to the tolerance, G2P) of the 64x32-cell variant:
     residual/tangent assembly scaled by the particle count, each sparse direct
-    solve by DOFs^1.5.  Returns (seconds, Newton iterations, description)."""
+    solve by DOFs^1.5.  threads: host threads for the tangent's complex-step
+    passes.  Returns (seconds, Newton iterations, description)."""
     import scipy.sparse.linalg as sla
     from . import mpm as M
     kw = dict(n_cells_x=64, n_cells_y=32, footing_width=0.25)
     kw.update(footing_kwargs or {})
     o = footing_oracle(**kw)
+    o.threads = threads
     t_solve = [0.0]
     orig = M.spsolve
 
@@ -121,8 +123,9 @@ def oracle_load_step_sample(footing_kwargs=None, full=(256, 128), step=0):
     est = (total - t_solve[0]) * pr + t_solve[0] * dr ** 1.5
     desc = (f"one complete load step ({its} Newton iterations; residual + complex-step tangents "
             f"{total - t_solve[0]:.2f} s, SciPy spsolve {t_solve[0]:.3f} s) of load step {step} of the "
-            f"{kw['n_cells_x']}x{kw['n_cells_y']}-cell variant ({o.N} particles, {o.ndof} DOFs), NumPy oracle on "
-            f"1 host thread; scaled to the 256x128-cell workload by x{pr:.0f} (particles) and x{dr ** 1.5:.0f} (solve)")
+            f"{kw['n_cells_x']}x{kw['n_cells_y']}-cell variant ({o.N} particles, {o.ndof} DOFs), NumPy oracle with "
+            f"{threads} host thread(s) for the tangent passes (SciPy's direct solve on one); scaled to the 256x128-cell "
+            f"workload by x{pr:.0f} (particles) and x{dr ** 1.5:.0f} (solve)")
     return est, its, desc
 
 
@@ -156,13 +159,14 @@ def consolidation_boundary_np(boundary, n_grid_x, n_grid_y):
     boundary[dof[iy <= 0] + nn] = True
 
 
-def oracle_consolidation_sample(dicts, dts, max_steps=20, budget_s=15.0):
+def oracle_consolidation_sample(dicts, dts, max_steps=20, budget_s=15.0, threads=1):
     """Seconds per load step of the full consolidation column in the oracle:
     consecutive load steps from the start of the schedule (P2G, Newton to the
     tolerance with a SciPy sparse direct solve, G2P) until max_steps or
     budget_s.  Returns (seconds per step, steps run, description)."""
     grid, parts, it, mat, porous, load = dicts
     o = consolidation_oracle(grid, parts, it, mat, porous, load)
+    o.threads = threads
     bnd = lambda b: consolidation_boundary_np(b, grid["n_grid_x"], grid["n_grid_y"])
     t0 = time.perf_counter()
     n = 0
@@ -173,7 +177,7 @@ def oracle_consolidation_sample(dicts, dts, max_steps=20, budget_s=15.0):
     sec = (time.perf_counter() - t0) / n
     desc = (f"load steps 0..{n - 1} of the full column ({o.N} particles, {o.ndof} DOFs; "
             f"{sum(o.iters) / n:.1f} Newton iterations per step, complex-step tangents and SciPy spsolve), "
-            f"NumPy oracle on 1 host thread")
+            f"NumPy oracle with {threads} host thread(s) for the tangent passes")
     return sec, n, desc
 
 
@@ -202,12 +206,13 @@ def bar_oracle(width_cells=4, height_cells=40, dx=0.25, PPD=2, E=1e6, nu=0.3, rh
     return o
 
 
-def oracle_bar_sample(n_steps=50, max_steps=50, budget_s=15.0):
+def oracle_bar_sample(n_steps=50, max_steps=50, budget_s=15.0, threads=1):
     """Seconds per load step of the self-weight bar in the oracle:
     consecutive load steps from the start (P2G, Newton with a SciPy sparse
     direct solve, G2P) until max_steps or budget_s.  Returns (seconds per
     step, steps run, description)."""
     o = bar_oracle()
+    o.threads = threads
     t0 = time.perf_counter()
     n = 0
     while n < min(max_steps, n_steps) and time.perf_counter() - t0 < budget_s:
@@ -215,5 +220,6 @@ def oracle_bar_sample(n_steps=50, max_steps=50, budget_s=15.0):
         n += 1
     sec = (time.perf_counter() - t0) / n
     desc = (f"load steps 0..{n - 1} of the bar ({o.N} particles, {o.ndof} DOFs; {sum(o.iters) / n:.1f} Newton "
-            f"iterations per step, complex-step tangents and SciPy spsolve), NumPy oracle on 1 host thread")
+            f"iterations per step, complex-step tangents and SciPy spsolve), NumPy oracle with {threads} host "
+            f"thread(s) for the tangent passes")
     return sec, n, desc

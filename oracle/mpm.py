@@ -191,6 +191,7 @@ class OracleEngine:
     def __init__(self, kind, grid, x, p_vol, p_rho, PPD, mat, load, lp0, n_iter=10, tol=1e-8, dt=0.0,
                  phi_initial=0.0, mobility=0.0, E_field=None, act_thresh=None):
         self.kind = kind
+        self.threads = 1  # host threads for the tangent's complex-step passes (timing runs raise it)
         self.D = 2 if kind in ("solid2d", "coupled2d") else 3
         self.nf = {"solid2d": 2, "coupled2d": 3, "coupled3d": 4}[kind]
         self.grid = dict(grid)
@@ -438,18 +439,29 @@ class OracleEngine:
         np.add.at(R, dofs[okd], np.real(r)[okd])
         K = None
         if want_K:
-            rows, cols, vals = [], [], []
-            for b in range(A):
-                for g in range(self.nf):
-                    Up = Un.astype(np.complex128)
-                    Up[:, b, g] += 1j * CS_H
-                    rp = self.local(Up, Uo, geo, step, n_steps)
-                    dcol = -np.imag(rp) / CS_H  # K = -dR/du, column (b, g)
-                    colok = valid[:, b] & free[np.where(valid[:, b], dofs[:, b, g], 0)]
-                    m = okd & colok[:, None, None]
-                    rows.append(dofs[m])
-                    cols.append(np.broadcast_to(dofs[:, b, g][:, None, None], dofs.shape)[m])
-                    vals.append(dcol[m])
+            def column(bg):
+                # complex-step pass for local column (b, g): K = -dR/du
+                b, g = bg
+                Up = Un.astype(np.complex128)
+                Up[:, b, g] += 1j * CS_H
+                rp = self.local(Up, Uo, geo, step, n_steps)
+                dcol = -np.imag(rp) / CS_H
+                colok = valid[:, b] & free[np.where(valid[:, b], dofs[:, b, g], 0)]
+                m = okd & colok[:, None, None]
+                return (dofs[m], np.broadcast_to(dofs[:, b, g][:, None, None], dofs.shape)[m], dcol[m])
+
+            passes = [(b, g) for b in range(A) for g in range(self.nf)]
+            if self.threads > 1:
+                # the passes are independent NumPy work (the GIL is released in
+                # it); results are kept in pass order, so K is the same
+                from concurrent.futures import ThreadPoolExecutor
+                with ThreadPoolExecutor(self.threads) as ex:
+                    parts = list(ex.map(column, passes))
+            else:
+                parts = [column(bg) for bg in passes]
+            rows = [r for r, _, _ in parts]
+            cols = [c for _, c, _ in parts]
+            vals = [v for _, _, v in parts]
             nf_rows = np.where(~free)[0]
             rows.append(nf_rows)
             cols.append(nf_rows)
