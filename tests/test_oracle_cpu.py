@@ -161,3 +161,16 @@ def test_geostatic_state_inverts_hencky_and_is_in_equilibrium():
     R, _, _ = o.assemble(0, 100, want_K=False)
     weight = rho * g * parts["p_vol"] * parts["n_particles"]
     assert np.linalg.norm(R) < 1e-9 * weight
+
+
+def test_threaded_tangent_passes_give_the_same_jacobian():
+    """The oracle's complex-step passes on several host threads (the timing
+    runs) assemble exactly the residual and Jacobian of the serial passes."""
+    from oracle.bench_sample import footing_oracle
+    o = footing_oracle(n_cells_x=16, n_cells_y=8, footing_width=0.25)
+    o.p2g()
+    R1, K1, _ = o.assemble(0, 100)
+    o.threads = 4
+    R2, K2, _ = o.assemble(0, 100)
+    assert np.array_equal(R1, R2)
+    assert (K1 != K2).nnz == 0 and K1.nnz == K2.nnz
