@@ -1,21 +1,25 @@
-"""Benchmark: load steps/s of the implicit cpGIMP engine on the plane-strain
-Drucker-Prager strip footing (256 x 128 soil cells, 2 x 2 particles per cell
-= 131,072 particles, 1 m footing pushed 0.2 m over 100 load steps).
+"""Benchmark: block load steps/s (forward + adjoint) of the implicit cpGIMP
+engine on the batched inverse analysis: 64 self-weight soil blocks of
+32x32..128x64 cells (seeded), 2 x 2 particles per cell (1,002,044 particles),
+per-particle log Young's modulus from a Gaussian random field, packed into
+one engine; the loss is the L2 misfit to the displacements a second field
+produces, and every step also runs the hand-written adjoint of the load step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl geowarp|reference]
 
-One "step" is one load step: P2G (cell sort, activation, pattern), the Newton
-loop (residual + exact element tangent, GMRES on the block-CSR Jacobian) and
-G2P, followed by its adjoint (transpose solve with the converged Jacobian and
-the adjoint P2G/G2P), in the mixed FP32/FP64 mode.  The plain FP64 engine runs
-the same steps for the error check and is reported beside it.  With N GPUs
-the job runs N independent replicas (one per rank; there is no data-path
-collective) and `value` is the aggregate over ranks.
+One "step" is one load step of all 64 blocks: P2G (cell sort, activation,
+pattern), the Newton loop (residual + exact element tangent, GMRES on the
+block-CSR Jacobian) and G2P, followed by its adjoint (transpose solve with the
+converged Jacobian and the adjoint P2G/G2P), in the mixed FP32/FP64 mode.  The
+plain FP64 engine runs the same steps for the error check and is reported
+beside it.  With N GPUs the job runs N independent replicas (one per rank;
+there is no data-path collective) and `value` is the aggregate over ranks.
 
---workload batched runs 64 inverse-analysis blocks packed into one engine;
---workload consolidation runs the 1 x 200-cell coupled u-p column (forward
-load steps with their own time increments; the adjoint covers the 2D solid
-solver); --workload bar runs the 4 x 40-cell self-weight bar.
+--workload footing runs the plane-strain Drucker-Prager strip footing (256 x
+128 cells, 131,072 particles); --workload consolidation runs the 1 x 200-cell
+coupled u-p column (forward load steps with their own time increments; the
+adjoint covers the 2D solid solver); --workload bar runs the 4 x 40-cell
+self-weight bar.
 
 Before the timed region, --autotune on (the default) searches the library's
 launch-shape knobs on the workload's own load step (geowarp_b200.autotune); the
@@ -55,8 +59,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="geowarp", choices=["geowarp", "reference"])
     ap.add_argument("--small", action="store_true", help="64x32-cell variant for quick checks")
-    ap.add_argument("--workload", default="footing", choices=["footing", "batched", "consolidation", "bar"],
-                    help="footing: the strip footing (default); batched: 64 inverse-analysis blocks in one engine; "
+    ap.add_argument("--workload", default="batched", choices=["footing", "batched", "consolidation", "bar"],
+                    help="batched: 64 inverse-analysis blocks in one engine (default); footing: the strip footing; "
                          "consolidation: the 1 x 200-cell u-p column (forward load steps); bar: the 4 x 40-cell "
                          "self-weight bar")
     ap.add_argument("--instances", type=int, default=64, help="blocks of the batched workload")
@@ -207,7 +211,7 @@ class BatchedWorkload(Workload):
         self.logE = batch.random_fields(self.sizes, seed=1000)
         self.logE_target = batch.random_fields(self.sizes, seed=2000)
         self.units = self.n
-        self.n_steps = 50
+        self.n_steps = N_STEPS_TOTAL
         self.targets = None
         npart = sum(a * b * 4 for a, b in self.sizes)
         self.config = dict(workload=f"batched inverse analysis: {self.n} self-weight blocks in one engine",
@@ -215,7 +219,7 @@ class BatchedWorkload(Workload):
                                  "cells between blocks", particles=npart, ppc="2x2",
                            material="Hencky elastic, nu=0.3, log E = Gaussian random field (mean ln 1e7, std 0.3, "
                                     "correlation length 0.5 m, seeds 1000+q); targets from a second field (seeds 2000+q)",
-                           load="self-weight rho=2000 kg/m3 g=9.81 ramped over 50 load steps",
+                           load=f"self-weight rho=2000 kg/m3 g=9.81 ramped over {N_STEPS_TOTAL} load steps",
                            units="value counts block load steps (blocks x load steps)")
         self.metric = METRIC.replace("load steps/s", "block load steps/s")
 
@@ -556,24 +560,26 @@ def oracle_rate(wl, steps=2, budget_s=15.0):
         from oracle.bench_sample import oracle_bar_sample
         sec, n, sample = oracle_bar_sample(wl.n_steps, max_steps=max(steps, 3), budget_s=budget_s, threads=th)
         return 1.0 / sec, th, sample + " (forward load steps; the CPU path has no adjoint)"
+    if isinstance(wl, BatchedWorkload):
+        # whole blocks of the batch, each a complete load step: the blocks are
+        # independent, so blocks per second is the metric's own unit
+        from oracle.bench_sample import oracle_batch_sample
+        rate, n, sample = oracle_batch_sample(wl.sizes, wl.logE, wl.n_steps, budget_s=budget_s, threads=th)
+        return rate, th, sample
     from oracle.bench_sample import oracle_load_step_sample
     times = []
     for k in range(max(1, min(steps, 2))):
         sec, its, sample = oracle_load_step_sample(step=k, threads=th)
         times.append(sec)
-    scale = 1.0
-    if isinstance(wl, BatchedWorkload):
-        # per-particle work dominates the oracle step: scale by particles
-        scale = wl.config["particles"] / 131072.0
-        sample += f"; scaled to the batch by x{scale:.2f} (particles)"
-    return wl.units / (float(np.mean(times)) * scale), th, sample + " (forward load step; the CPU path has no adjoint)"
+    return wl.units / float(np.mean(times)), th, sample + " (forward load step; the CPU path has no adjoint)"
 
 
 def cpu_baseline(wl, gpu_line):
-    """Oracle timing on a bounded sample, run on rank 0 (one load step of the
-    64x32-cell footing variant scaled to the workload, or the first load steps
-    of the bar / column)."""
-    v, th, sample = oracle_rate(wl, steps=1)
+    """Oracle timing on a bounded sample of the same workload, run on rank 0:
+    whole blocks of the batch (one load step each), the first load steps of
+    the bar / column, or one load step of the 64x32-cell footing variant
+    scaled to the full footing."""
+    v, th, sample = oracle_rate(wl, steps=1, budget_s=20.0)
     return {"value": v, "unit": gpu_line["unit"], "cores": th, "kind": "port", "sample": sample}
 
 

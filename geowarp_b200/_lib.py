@@ -92,6 +92,8 @@ SIGNATURES = {
     "gw_version": (C.c_int, []),
     "gw_status_string": (C.c_char_p, [C.c_int]),
     "gw_read_device_status": (C.c_int, [PI32, P]),
+    "gw_guard_read": (C.c_int, [PI32, C.POINTER(C.c_int64), P]),
+    "gw_guard_site_name": (C.c_char_p, [I32]),
     "gw_sort_workspace_bytes": (I64, [I32]),
     "gw_cell_sort": (C.c_int, [C.POINTER(Grid), C.POINTER(Particles), P, P, P, P]),
     "gw_p2g_activate": (C.c_int, [C.POINTER(Grid), C.POINTER(Particles), P, P, P, P, P]),

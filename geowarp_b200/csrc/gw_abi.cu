@@ -1,162 +1,35 @@
 // C ABI of the engine (declarations and reference citations in
-// include/geowarp_b200.h).  This is the library's single translation unit.
-#include <stddef.h>
-#include <stdio.h>
-#include <string.h>
-
-#include "gw_step_kernels.cuh"
-#include "gw_krylov.cuh"
+// include/geowarp_b200.h): queries, cell sort, activation, pattern,
+// consistent mass, norms, G2P, single-point models, launch knobs and kernel
+// timing.  The solvers, the assembly and the adjoint entry points live in
+// gw_abi_solve.cu, gw_abi_assemble.cu and gw_abi_adjoint.cu.  This file also
+// defines the device globals the kernel headers declare.
+#define GW_DEFINE_DEVICE_GLOBALS
+#include "gw_host.cuh"
 #include "gw_mg.cuh"
-#include "gw_adjoint.cuh"
 
 using namespace gw;
+using namespace gwh;
 
-namespace {
-
-thread_local char g_msg[512];
-
-#define GW_CUDA(call)                                                                         \
-    do {                                                                                      \
-        cudaError_t e_ = (call);                                                              \
-        if (e_ != cudaSuccess) {                                                              \
-            snprintf(g_msg, sizeof(g_msg), "%s:%d %s", __FILE__, __LINE__, cudaGetErrorString(e_)); \
-            return GW_ECUDA;                                                                  \
-        }                                                                                     \
-    } while (0)
-#define GW_LAUNCHED() GW_CUDA(cudaGetLastError())
-#define GW_REQUIRE(cond)                                                      \
-    do {                                                                      \
-        if (!(cond)) {                                                        \
-            snprintf(g_msg, sizeof(g_msg), "invalid argument: %s", #cond);    \
-            return GW_EINVAL;                                                 \
-        }                                                                     \
-    } while (0)
-
-inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
-
-// -------------------------------------------------------------- optional kernel timing
-// When enabled, selected launches are bracketed by CUDA events on their stream;
-// gw_profile_read() synchronises and reports per-class totals and the
-// algorithmic bytes the host attributed to each launch.
-enum ProfClass {
-    PC_ASSEMBLE = 0, PC_SPMV, PC_DOTS, PC_UPDATE, PC_NEXT, PC_G2P, PC_ADJ_G2P, PC_ADJ_RES,
-    PC_MG_JACOBI, PC_MG_RESID, PC_MG_TRANSFER, PC_MG_SETUP, PC_MG_JACOBI_COARSE, PC_COUNT
-};
-const char *kProfNames[PC_COUNT] = {"k_assemble", "k_gm_spmv", "k_gm_dots", "k_gm_update", "k_gm_next", "k_g2p",
-                                    "k_adjoint_g2p", "k_adjoint_residual", "k_mg_jacobi (finest level)",
-                                    "k_mg_residual", "k_mg_restrict/prolong", "mg_setup",
-                                    "k_mg_jacobi (coarse levels)"};
-struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
-bool g_prof_on = false;
-ProfRec *g_prof = nullptr;
-int g_prof_n = 0, g_prof_cap = 0;
-double g_prof_ms[PC_COUNT], g_prof_bytes[PC_COUNT];
-long g_prof_count[PC_COUNT];
-
-struct ProfScope {
-    ProfRec *r = nullptr;
-    cudaStream_t s;
-    ProfScope(int cls, cudaStream_t st, double bytes) : s(st) {
-        if (!g_prof_on) return;
-        if (g_prof_n == g_prof_cap) {
-            int nc = g_prof_cap ? 2 * g_prof_cap : 4096;
-            ProfRec *nr = (ProfRec *)realloc(g_prof, sizeof(ProfRec) * nc);
-            if (!nr) return;
-            g_prof = nr;
-            g_prof_cap = nc;
-        }
-        r = &g_prof[g_prof_n++];
-        r->cls = cls;
-        r->bytes = bytes;
-        cudaEventCreate(&r->a);
-        cudaEventCreate(&r->b);
-        cudaEventRecord(r->a, s);
-    }
-    ~ProfScope() {
-        if (r) cudaEventRecord(r->b, s);
-    }
-};
-// every kernel launch of the library passes its grid size through here, so the
-// host can report how many launches a piece of work took (gw_launch_count)
-int64_t g_launches = 0;
-inline int gw_count_launch(int grid) {
-    ++g_launches;
-    return grid;
-}
-inline int nblk(int64_t n, int t) { return (int)((n + t - 1) / t); }
-// The row kernels gather 2x2 and 4x4 blocks and their vectors with 16-byte
-// loads: those systems need 16-byte aligned values and vectors.
-inline bool aligned16(const void *p) { return ((uintptr_t)p & 15u) == 0; }
-inline bool vec_ok(const gw_bsr_t *A, const void *u, const void *v) {
-    if (A->nf != 2 && A->nf != 4) return true;
-    return aligned16(A->vals) && aligned16(u) && aligned16(v);
-}
-
-// launch-shape knobs (gw_tune_set): particle CTA, adjoint CTA, warps per CTA
-// of the multigrid row kernels, bound of the dense coarsest level
-int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160};
-inline int tune_rows_grid(int n_rows) {
-    const int w = g_tune[GW_TUNE_ROW_WARPS];
-    int b = nblk(n_rows, w);
-    return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b);
-}
-inline int tune_rows_block() { return 32 * g_tune[GW_TUNE_ROW_WARPS]; }
-inline int red_grid_rows(int n_rows) { int b = nblk(n_rows, kThreads / 32); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
-inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
-
-LaunchConst make_lc(const gw_grid_t *g, const gw_material_t *m, const gw_step_t *st) {
-    LaunchConst c;
-    memset(&c, 0, sizeof(c));
-    c.g = *g;
-    if (st) c.st = *st;
-    if (m) {
-        c.mc = make_matconst(*m);
-        c.E0 = m->youngs_modulus;
-        c.nu = m->poisson_ratio;
-    }
-    return c;
-}
-
-int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
-
-// -------------------------------------------------------------- exclusive scan
-int64_t scan_ws_ints(int64_t n) {
-    int64_t total = 0;
-    while (n > 1024) {
-        const int64_t nb = (n + 1023) / 1024;
-        total += 2 * nb + 64;
-        n = nb;
-    }
-    return total + 64;
-}
-
-int scan_exclusive(const int *in, int *out, int n, int *ws, cudaStream_t s) {
-    if (n <= 0) return GW_OK;
-    const int nb = (n + 1023) / 1024;
-    int *sums = ws;
-    int *sums_scan = ws + nb;
-    k_scan_block<<<gw_count_launch(nb), 1024, 0, s>>>(in, out, n, nb > 1 ? sums : nullptr);
-    GW_LAUNCHED();
-    if (nb > 1) {
-        int rc = scan_exclusive(sums, sums_scan, nb, ws + 2 * nb + 64, s);
-        if (rc) return rc;
-        k_scan_add<<<gw_count_launch(nb), 1024, 0, s>>>(out, n, sums_scan);
-        GW_LAUNCHED();
-    }
+extern "C" int gw_guard_read(int32_t *site, int64_t *value, void *stream) {
+    GW_REQUIRE(site && value);
+    int st = 0;
+    long long v = 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    GW_CUDA(cudaMemcpyFromSymbolAsync(&st, g_guard_site, sizeof(int), 0, cudaMemcpyDeviceToHost, s));
+    GW_CUDA(cudaMemcpyFromSymbolAsync(&v, g_guard_value, sizeof(long long), 0, cudaMemcpyDeviceToHost, s));
+    GW_CUDA(cudaStreamSynchronize(s));
+    const int zero = 0;
+    GW_CUDA(cudaMemcpyToSymbolAsync(g_guard_site, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+    GW_CUDA(cudaStreamSynchronize(s));
+    *site = st;
+    *value = v;
     return GW_OK;
 }
 
-__global__ void k_add2(const int *a, const int *b, int *out) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *out = *a + *b;
+extern "C" const char *gw_guard_site_name(int32_t site) {
+    return (site >= 0 && site < GS_COUNT) ? kGuardNames[site] : "unknown site";
 }
-
-int n_cells_of(const gw_grid_t &g) {
-    int c = 1;
-    for (int k = 0; k < g.dim; ++k) c *= g.n_grid[k];
-    return c;
-}
-
-}  // namespace
 
 // ==================================================================== queries
 extern "C" int gw_version(void) { return 1; }
@@ -359,1043 +232,6 @@ extern "C" int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_
     return GW_OK;
 }
 
-// ==================================================================== residual + Jacobian
-namespace {
-template <int KIND, typename VT>
-void assemble_per_model(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
-                        const double *uo, const PtrsA &a, double *R, double *force, int b, cudaStream_t s) {
-    const int pb = g_tune[GW_TUNE_PARTICLE_BLOCK];
-    switch (c.mc.model) {
-        case GW_MODEL_HENCKY: k_assemble<KIND, true, VT, GW_MODEL_HENCKY><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_J2: k_assemble<KIND, true, VT, GW_MODEL_J2><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_NEOHOOKEAN: k_assemble<KIND, true, VT, GW_MODEL_NEOHOOKEAN><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_LINEAR: k_assemble<KIND, true, VT, GW_MODEL_LINEAR><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        case GW_MODEL_DP: k_assemble<KIND, true, VT, GW_MODEL_DP><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-        default: k_assemble<KIND, true, VT><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force); break;
-    }
-}
-
-template <int KIND>
-int launch_assemble(const LaunchConst &c, const PtrsP &p, const int *perm, const uint8_t *fm, const double *un,
-                    const double *uo, const gw_bsr_t *A, int prec, double *R, double *force, const PtrsA &a,
-                    cudaStream_t s) {
-    const int pb = g_tune[GW_TUNE_PARTICLE_BLOCK];
-    const int b = nblk(p.n, pb);
-    if (p.n > 0) {
-        const int D = KindTraits<KIND>::D, NF = KindTraits<KIND>::NF, NS = KindTraits<KIND>::NS;
-        // algorithmic bytes, each array once: particle state in (x, lp, F_old,
-        // b_old, E) and out (F_new, b_new, sigma), the grid vectors (u_new, u_old,
-        // R) and the matrix values
-        (void)NS;
-        const double per_p = 8.0 * (2 * D + 9 + 9 + 1) + 8.0 * 27;
-        const double grid = 8.0 * 3 * (double)A->n_rows * NF;
-        const bool want_K = A->vals != nullptr;
-        const double mat = want_K ? (double)A->nnzb * NF * NF * (prec == GW_PREC_F64 ? 8 : 4) : 0.0;
-        ProfScope ps(PC_ASSEMBLE, s, per_p * p.n + grid + mat);
-        if (!want_K) {
-            k_assemble<KIND, false, double><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-        } else if constexpr (KIND == GW_KIND_SOLID2D) {
-            // the 2D solid tangent kernel is instantiated per material, so each
-            // carries only its own constitutive code (fewer registers and spills)
-            if (prec == GW_PREC_F64) assemble_per_model<KIND, double>(c, p, perm, fm, un, uo, a, R, force, b, s);
-            else assemble_per_model<KIND, float>(c, p, perm, fm, un, uo, a, R, force, b, s);
-        } else {
-            if (prec == GW_PREC_F64) k_assemble<KIND, true, double><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-            else k_assemble<KIND, true, float><<<gw_count_launch(b), pb, 0, s>>>(c, p, perm, fm, un, uo, a, R, force);
-        }
-        GW_LAUNCHED();
-    }
-    if (A->vals && A->n_rows > 0) {
-        const int D = KindTraits<KIND>::D;
-        if (prec == GW_PREC_F64) k_identity_dirichlet<D, double><<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, s>>>(a, fm);
-        else k_identity_dirichlet<D, float><<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, s>>>(a, fm);
-        GW_LAUNCHED();
-    }
-    return GW_OK;
-}
-}  // namespace
-
-extern "C" int gw_assemble(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
-                           const gw_particles_t *pt, const int32_t *perm, const uint8_t *free_mask,
-                           const double *u_new, const double *u_old, const gw_bsr_t *A, int32_t prec, double *R_rows,
-                           double *force, void *stream) {
-    GW_REQUIRE(grid && mat && st && pt && perm && free_mask && u_new && u_old && R_rows);
-    // the row map is needed for the residual even without a matrix
-    GW_REQUIRE(A && A->node2row && (A->n_rows == 0 || A->row2node));
-    GW_REQUIRE(mat->model >= 0 && mat->model <= GW_MODEL_NORSAND);
-    cudaStream_t s = S(stream);
-    LaunchConst c = make_lc(grid, mat, st);
-    PtrsP p = make_ptrs(*pt);
-    PtrsA a = make_ptrs(*A);
-    if (A->vals) {
-        GW_REQUIRE(A->row_ptr && A->cols && A->stencil);
-        const size_t vb = (prec == GW_PREC_F64 ? 8 : 4) * (size_t)A->nnzb * A->nf * A->nf;
-        GW_CUDA(cudaMemsetAsync(A->vals, 0, vb, s));
-    }
-    GW_CUDA(cudaMemsetAsync(R_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
-    switch (grid->kind) {
-        case GW_KIND_SOLID2D: return launch_assemble<GW_KIND_SOLID2D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
-        case GW_KIND_COUPLED2D: return launch_assemble<GW_KIND_COUPLED2D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
-        case GW_KIND_COUPLED3D: return launch_assemble<GW_KIND_COUPLED3D>(c, p, perm, free_mask, u_new, u_old, A, prec, R_rows, force, a, s);
-        default: return GW_EINVAL;
-    }
-}
-
-// ==================================================================== Krylov
-namespace {
-struct KWs {
-    double *r, *rh, *p, *v, *y, *s, *z, *t, *Minv, *partials;
-    KScalars *sc;
-};
-
-int64_t krylov_ws_bytes(int64_t n_rows, int nf) {
-    const int64_t n = n_rows * nf;
-    return 8 * align256(8 * n) + align256(8 * n_rows * nf * nf) + align256(8 * (int64_t)kRedBlocks * 4) +
-           align256(sizeof(KScalars));
-}
-
-KWs carve(void *ws, int64_t n_rows, int nf) {
-    const int64_t n = n_rows * nf;
-    char *w = (char *)ws;
-    KWs k;
-    double **vecs[8] = {&k.r, &k.rh, &k.p, &k.v, &k.y, &k.s, &k.z, &k.t};
-    for (int i = 0; i < 8; ++i) { *vecs[i] = (double *)w; w += align256(8 * n); }
-    k.Minv = (double *)w; w += align256(8 * n_rows * nf * nf);
-    k.partials = (double *)w; w += align256(8 * (int64_t)kRedBlocks * 4);
-    k.sc = (KScalars *)w;
-    return k;
-}
-
-template <int NF, typename VT>
-int krylov(const gw_bsr_t *A, int method, int precond, const double *b, double *x, double rtol, int max_iter, void *ws,
-           int *iters, double *relres, cudaStream_t s) {
-    PtrsA a = make_ptrs(*A);
-    KWs k = carve(ws, A->n_rows, NF);
-    const int D = (A->mask_words == 1) ? 2 : 3;
-    const int nr = A->n_rows;
-    if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
-    BicgVecs V;
-    V.x = x; V.b = b; V.r = k.r; V.rh = k.rh; V.p = k.p; V.v = k.v; V.y = k.y; V.s = k.s; V.z = k.z; V.t = k.t;
-    V.Minv = k.Minv; V.partials = k.partials; V.sc = k.sc;
-    GW_CUDA(cudaMemsetAsync(k.sc, 0, sizeof(KScalars), s));
-    KScalars h;
-    memset(&h, 0, sizeof(h));
-    h.max_iter = max_iter;
-    GW_CUDA(cudaMemcpyAsync(&k.sc->max_iter, &h.max_iter, sizeof(int), cudaMemcpyHostToDevice, s));
-    k_precond_setup<NF, VT><<<gw_count_launch(nblk(nr, kThreads)), kThreads, 0, s>>>(a, D, precond, k.Minv);
-    GW_LAUNCHED();
-    const int gw_rows = red_grid_rows(nr), ge_rows = red_grid_elems(nr);
-    if (method == GW_KRYLOV_CG) k_cg_init<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V, rtol);
-    else k_bicg_init<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V, rtol);
-    GW_LAUNCHED();
-    int chunk = 2;
-    for (;;) {
-        GW_CUDA(cudaMemcpyAsync(&h, k.sc, sizeof(KScalars), cudaMemcpyDeviceToHost, s));
-        GW_CUDA(cudaStreamSynchronize(s));
-        if (h.done) break;
-        for (int it = 0; it < chunk; ++it) {
-            if (method == GW_KRYLOV_CG) {
-                k_cg_p<NF><<<gw_count_launch(red_grid_elems((int64_t)nr * NF)), kThreads, 0, s>>>(nr, V);
-                k_cg_q<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V);
-                k_cg_xr<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
-            } else {
-                k_bicg_p<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
-                k_bicg_v<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V);
-                k_bicg_s<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
-                k_bicg_t<NF, VT><<<gw_count_launch(gw_rows), kThreads, 0, s>>>(a, V);
-                k_bicg_xr<NF><<<gw_count_launch(ge_rows), kThreads, 0, s>>>(nr, V);
-            }
-        }
-        GW_LAUNCHED();
-        chunk = chunk < 64 ? chunk * 2 : 64;
-    }
-    *iters = h.iters;
-    *relres = (h.bb > 0.0) ? ::sqrt(h.rr / h.bb) : 0.0;
-    if (h.status == ST_BREAKDOWN) return GW_EBREAKDOWN;
-    if (h.status == ST_NAN) return GW_ENAN;
-    if (h.rr > h.tol2) return GW_ENOCONV;
-    return GW_OK;
-}
-
-template <typename VT>
-int krylov_nf(const gw_bsr_t *A, int method, int precond, const double *b, double *x, double rtol, int max_iter,
-              void *ws, int *iters, double *relres, cudaStream_t s) {
-    switch (A->nf) {
-        case 1: return krylov<1, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
-        case 2: return krylov<2, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
-        case 3: return krylov<3, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
-        case 4: return krylov<4, VT>(A, method, precond, b, x, rtol, max_iter, ws, iters, relres, s);
-        default: return GW_EINVAL;
-    }
-}
-}  // namespace
-
-namespace {
-int64_t gmres_ws_bytes(int64_t n_rows, int nf, int restart) {
-    const int64_t n = n_rows * nf;
-    return align256(8 * n * (restart + 1)) + 2 * align256(8 * n) + align256(8 * n_rows * nf * nf) +
-           align256(8 * (int64_t)kRedBlocks * (kGmresMaxRestart + 1)) + align256(sizeof(GScalars));
-}
-
-template <int NF, typename VT>
-int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rtol, int max_iter, int restart,
-          void *ws, int *iters, double *relres, cudaStream_t s) {
-    PtrsA a = make_ptrs(*A);
-    const int nr = A->n_rows;
-    if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
-    const int64_t n = (int64_t)nr * NF;
-    char *w = (char *)ws;
-    GmresVecs G;
-    G.V = (double *)w; w += align256(8 * n * (restart + 1));
-    G.w = (double *)w; w += align256(8 * n);
-    G.z = (double *)w; w += align256(8 * n);
-    G.Minv = (double *)w; w += align256(8 * (int64_t)nr * NF * NF);
-    G.partials = (double *)w; w += align256(8 * (int64_t)kRedBlocks * (kGmresMaxRestart + 1));
-    G.sc = (GScalars *)w;
-    G.x = x; G.b = b; G.n = (size_t)n;
-    const size_t head = offsetof(GScalars, H);
-    GW_CUDA(cudaMemsetAsync(G.sc, 0, head, s));
-    struct { int max_iter, restart; } lim = {max_iter, restart};
-    GW_CUDA(cudaMemcpyAsync(&G.sc->max_iter, &lim, sizeof(lim), cudaMemcpyHostToDevice, s));
-    const int D = (A->mask_words == 1) ? 2 : 3;
-    k_precond_setup<NF, VT><<<gw_count_launch(nblk(nr, kThreads)), kThreads, 0, s>>>(a, D, precond, G.Minv);
-    GW_LAUNCHED();
-    const int gr = red_grid_rows(nr), ge = red_grid_elems(nr), gv = red_grid_elems(n);
-    GScalars h;
-    memset(&h, 0, head);
-    int first = 1;
-    for (int cycle = 0; cycle < 1000000; ++cycle) {
-        k_gm_residual<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, first, rtol);
-        k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 1);
-        GW_LAUNCHED();
-        first = 0;
-        GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
-        GW_CUDA(cudaStreamSynchronize(s));
-        if (h.done) break;
-        int chunk = 4;
-        int kk = 0;  // host-side column estimate (exact until the cycle closes early)
-        const double spmv_bytes = (double)A->nnzb * (NF * NF * sizeof(VT) + 4) + 4.0 * (nr + 1) + 16.0 * n;
-        for (;;) {
-            for (int it = 0; it < chunk; ++it, ++kk) {
-                const double vb = 8.0 * n * (kk + 2);
-                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_NEXT, s, 8.0 * n * 3 + 8.0 * nr * NF * NF); k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 0); }
-            }
-            GW_LAUNCHED();
-            GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
-            GW_CUDA(cudaStreamSynchronize(s));
-            if (h.cycle_done) break;
-            chunk = chunk < 32 ? chunk * 2 : 32;
-        }
-        if (h.status) break;
-        k_gm_solve_y<<<gw_count_launch(1), 32, 0, s>>>(G.sc);
-        k_gm_update_x<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G);
-        GW_LAUNCHED();
-    }
-    *iters = h.iters;
-    *relres = (h.bnorm > 0.0) ? h.resid / h.bnorm : 0.0;
-    if (h.status == ST_NAN) return GW_ENAN;
-    if (h.resid > h.tol) return GW_ENOCONV;
-    return GW_OK;
-}
-
-template <typename VT>
-int gmres_nf(const gw_bsr_t *A, int precond, const double *b, double *x, double rtol, int max_iter, int restart,
-             void *ws, int *iters, double *relres, cudaStream_t s) {
-    switch (A->nf) {
-        case 1: return gmres<1, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
-        case 2: return gmres<2, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
-        case 3: return gmres<3, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
-        case 4: return gmres<4, VT>(A, precond, b, x, rtol, max_iter, restart, ws, iters, relres, s);
-        default: return GW_EINVAL;
-    }
-}
-}  // namespace
-
-extern "C" int64_t gw_gmres_workspace_bytes(int32_t n_rows, int32_t nf, int32_t restart) {
-    if (restart < 1 || restart > kGmresMaxRestart) return -1;
-    return gmres_ws_bytes(n_rows, nf, restart);
-}
-
-extern "C" int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const double *b, double *x,
-                                  double rtol, int32_t max_iter, int32_t restart, void *workspace, int32_t *iters_host,
-                                  double *relres_host, void *stream) {
-    GW_REQUIRE(A && b && x && workspace && iters_host && relres_host && max_iter > 0);
-    GW_REQUIRE(vec_ok(A, b, x));
-    GW_REQUIRE(restart >= 1 && restart <= kGmresMaxRestart);
-    int it = 0;
-    double rr = 0.0;
-    int rc = (prec == GW_PREC_F64)
-                 ? gmres_nf<double>(A, precond, b, x, rtol, max_iter, restart, workspace, &it, &rr, S(stream))
-                 : gmres_nf<float>(A, precond, b, x, rtol, max_iter, restart, workspace, &it, &rr, S(stream));
-    *iters_host = it;
-    *relres_host = rr;
-    return rc;
-}
-
-// ==================================================================== multigrid-preconditioned flexible GMRES
-namespace {
-constexpr double kMgOmega = 0.7;  // damping of the block-Jacobi smoother
-// smoothing sweeps before / after the coarse correction on every level (one
-// sweep on the coarse levels saves launches but costs FP64 Krylov iterations)
-inline int mg_sweeps(int) { return 2; }
-
-// Bump allocator over the caller's workspace; with p == nullptr it only counts,
-// so sizing and carving run the same code.
-struct Bump {
-    char *p;
-    int64_t used;
-    void *take(int64_t b) {
-        b = align256(b);
-        void *r = p ? (void *)(p + used) : nullptr;
-        used += b;
-        return r;
-    }
-};
-
-struct MgLevel {
-    gw_grid_t g;
-    Lat L;
-    gw_bsr_t A;             // level 0: the caller's matrix; coarse levels: FP64 in the workspace
-    double *Minv, *b, *x, *x2, *r;
-    uint8_t *fixed;
-    int *tmp, *sws, *blockrow;
-    uint8_t *flags;
-};
-struct MgHier {
-    int nl = 0;             // levels holding a matrix; the last one is solved with a dense inverse
-    MgLevel lv[kMgMaxLevels];
-    double *dM = nullptr, *dInv = nullptr;
-    int dn = 0;
-};
-
-gw_grid_t coarse_grid(const gw_grid_t &g) {
-    gw_grid_t c = g;
-    int nn = 1;
-    for (int k = 0; k < 3; ++k) {
-        if (k < g.dim) {
-            c.n_grid[k] = (g.n_grid[k] + 1) / 2;  // fine nodes N -> coarse nodes N/2 + 1
-            nn *= c.n_grid[k] + 1;
-        } else {
-            c.n_grid[k] = 0;
-        }
-        c.h[k] = 2.0 * g.h[k];
-        c.inv_h[k] = 0.5 * g.inv_h[k];
-        c.h_nodes[k] = 2.0 * g.h_nodes[k];
-    }
-    c.n_nodes = nn;
-    return c;
-}
-
-// Carves (or, with a counting Bump, sizes) every level of the hierarchy at its
-// upper bound -- a coarse level holds at most its lattice's node count of rows
-// and 5^D blocks per row -- and then the flexible-GMRES vectors.  The hierarchy
-// comes first, so its addresses depend only on (grid, n_rows, nf): a plan built
-// in a workspace stays valid for any restart length.
-struct FlexVecs {
-    double *V, *Z, *w, *partials;
-    GScalars *sc;
-};
-void mg_carve_hier(Bump &bp, MgHier &h, const gw_grid_t &g0, int64_t n_rows0, int nf) {
-    const int64_t n0 = n_rows0 * nf;
-    const int D = g0.dim, mw = D == 2 ? 1 : 4, S = D == 2 ? 25 : 125;
-    MgLevel &l0 = h.lv[0];
-    l0.g = g0;
-    l0.Minv = (double *)bp.take(8 * n_rows0 * nf * nf);
-    l0.b = (double *)bp.take(8 * n0);
-    l0.x = (double *)bp.take(8 * n0);
-    l0.x2 = (double *)bp.take(8 * n0);
-    l0.r = (double *)bp.take(8 * n0);
-    l0.fixed = (uint8_t *)bp.take(n_rows0);
-    gw_grid_t g = g0;
-    int64_t nodes = g0.n_nodes;
-    int l = 0;
-    // levels carved for the smallest coarsest-level bound a caller may set
-    for (; l + 1 < kMgMaxLevels && nodes * nf > kMgCoarseMin; ++l) {
-        g = coarse_grid(g);
-        nodes = g.n_nodes;
-        MgLevel &c = h.lv[l + 1];
-        c.g = g;
-        c.A.node2row = (int *)bp.take(4 * nodes);
-        c.A.row2node = (int *)bp.take(4 * nodes);
-        c.A.row_ptr = (int *)bp.take(4 * (nodes + 1));
-        c.A.stencil = (uint32_t *)bp.take(4 * nodes * mw);
-        c.A.cols = (int *)bp.take(4 * nodes * S);
-        c.A.vals = bp.take(8 * nodes * S * nf * nf);
-        c.blockrow = (int *)bp.take(4 * nodes * S);
-        c.tmp = (int *)bp.take(4 * (nodes + 1));
-        c.sws = (int *)bp.take(4 * (scan_ws_ints(nodes + 1) + 64));
-        c.flags = (uint8_t *)bp.take(nodes);
-        c.Minv = (double *)bp.take(8 * nodes * nf * nf);
-        c.b = (double *)bp.take(8 * nodes * nf);
-        c.x = (double *)bp.take(8 * nodes * nf);
-        c.x2 = (double *)bp.take(8 * nodes * nf);
-        c.r = (double *)bp.take(8 * nodes * nf);
-        c.fixed = (uint8_t *)bp.take(nodes);
-    }
-    h.nl = l + 1;  // upper bound; the plan may stop earlier
-    h.dM = (double *)bp.take(8 * (int64_t)kMgCoarseMax * kMgCoarseMax);
-    h.dInv = (double *)bp.take(8 * (int64_t)kMgCoarseMax * kMgCoarseMax);
-}
-void mg_carve_flex(Bump &bp, FlexVecs &fv, int64_t n0, int restart) {
-    fv.V = (double *)bp.take(8 * n0 * (restart + 1));
-    fv.Z = (double *)bp.take(8 * n0 * restart);
-    fv.w = (double *)bp.take(8 * n0);
-    fv.partials = (double *)bp.take(8 * (int64_t)kRedBlocks * (kGmresMaxRestart + 1));
-    fv.sc = (GScalars *)bp.take(sizeof(GScalars));
-}
-
-int64_t mg_ws_bytes(const gw_grid_t &g0, int64_t n_rows, int nf, int restart) {
-    Bump bp{nullptr, 0};
-    MgHier h;
-    FlexVecs fv;
-    mg_carve_hier(bp, h, g0, n_rows, nf);
-    mg_carve_flex(bp, fv, n_rows * nf, restart);
-    return bp.used;
-}
-
-// Pattern phase: the coarse active sets, row maps, stencils, row pointers and
-// columns of every level below A0 (two host reads per coarse level: its row
-// count and its block count).  Depends on A0's pattern only.
-template <int NF>
-int mg_pattern(MgHier &h, const gw_bsr_t *A0, gw_mg_plan_t *plan, cudaStream_t s) {
-    const int D = h.lv[0].g.dim, mw = D == 2 ? 1 : 4;
-    const int nl_bound = h.nl;
-    h.lv[0].L = lat_of(h.lv[0].g);
-    h.lv[0].A = *A0;
-    int l = 0;
-    while (h.lv[l].A.n_rows * NF > g_tune[GW_TUNE_MG_COARSE]) {
-        if (l + 1 >= nl_bound) {
-            snprintf(g_msg, sizeof(g_msg), "multigrid: coarsest level still has %d unknowns", h.lv[l].A.n_rows * NF);
-            return GW_EINVAL;
-        }
-        MgLevel &f = h.lv[l], &c = h.lv[l + 1];
-        c.L = lat_of(c.g);
-        const int N = c.g.n_nodes;
-        PtrsA fa = make_ptrs(f.A);
-        GW_CUDA(cudaMemsetAsync(c.flags, 0, N, s));
-        k_mg_coarse_flags<<<gw_count_launch(nblk(f.A.n_rows, kThreads)), kThreads, 0, s>>>(f.L, fa, c.L, c.flags);
-        k_flags_to_int<<<gw_count_launch(nblk(N, kThreads)), kThreads, 0, s>>>(c.flags, N, c.tmp);
-        GW_LAUNCHED();
-        GW_CUDA(cudaMemcpyAsync(c.sws, c.tmp + (N - 1), 4, cudaMemcpyDeviceToDevice, s));
-        int rc = scan_exclusive(c.tmp, c.tmp, N, c.sws + 64, s);
-        if (rc) return rc;
-        k_compact<<<gw_count_launch(nblk(N, kThreads)), kThreads, 0, s>>>(c.flags, c.tmp, N, NF, nullptr,
-                                                                          (int *)c.A.node2row, (int *)c.A.row2node, nullptr);
-        k_add2<<<gw_count_launch(1), 32, 0, s>>>(c.tmp + (N - 1), c.sws, c.sws + 1);
-        GW_LAUNCHED();
-        int nrc = 0;
-        GW_CUDA(cudaMemcpyAsync(&nrc, c.sws + 1, 4, cudaMemcpyDeviceToHost, s));
-        GW_CUDA(cudaStreamSynchronize(s));
-        if (nrc <= 0) {
-            snprintf(g_msg, sizeof(g_msg), "multigrid: empty coarse level");
-            return GW_EINVAL;
-        }
-        GW_CUDA(cudaMemsetAsync((void *)c.A.stencil, 0, 4 * (size_t)N * mw, s));
-        GW_CUDA(cudaMemsetAsync(c.tmp, 0, 4 * ((size_t)nrc + 1), s));
-        if (D == 2)
-            k_mg_coarse_stencil<2><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(
-                f.L, fa, c.L, nrc, c.A.row2node, (uint32_t *)c.A.stencil, mw, c.tmp);
-        else
-            k_mg_coarse_stencil<3><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(
-                f.L, fa, c.L, nrc, c.A.row2node, (uint32_t *)c.A.stencil, mw, c.tmp);
-        GW_LAUNCHED();
-        rc = scan_exclusive(c.tmp, (int *)c.A.row_ptr, nrc + 1, c.sws, s);
-        if (rc) return rc;
-        int nnzb = 0;
-        GW_CUDA(cudaMemcpyAsync(&nnzb, c.A.row_ptr + nrc, 4, cudaMemcpyDeviceToHost, s));
-        GW_CUDA(cudaStreamSynchronize(s));
-        c.A.n_rows = nrc;
-        c.A.nf = NF;
-        c.A.nnzb = nnzb;
-        c.A.mask_words = mw;
-        PtrsA ca = make_ptrs(c.A);
-        if (D == 2) k_pattern_fill<2><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(c.g, ca, (int *)c.A.cols);
-        else k_pattern_fill<3><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(c.g, ca, (int *)c.A.cols);
-        k_mg_blockrow<<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(c.A.row_ptr, nrc, c.blockrow);
-        GW_LAUNCHED();
-        ++l;
-    }
-    h.nl = l + 1;
-    h.dn = h.lv[l].A.n_rows * NF;
-    memset(plan, 0, sizeof(*plan));
-    plan->levels = h.nl;
-    plan->dense_n = h.dn;
-    for (int q = 0; q < h.nl; ++q) {
-        plan->n_rows[q] = h.lv[q].A.n_rows;
-        plan->nnzb[q] = h.lv[q].A.nnzb;
-    }
-    plan->nf = NF;
-    plan->fine_n_rows = A0->n_rows;
-    plan->fine_nnzb = A0->nnzb;
-    return GW_OK;
-}
-
-// Restores the level sizes a plan recorded into a freshly carved hierarchy.
-void mg_apply_plan(MgHier &h, const gw_bsr_t *A0, const gw_mg_plan_t *plan, int nf) {
-    const int mw = h.lv[0].g.dim == 2 ? 1 : 4;
-    h.nl = plan->levels;
-    h.dn = plan->dense_n;
-    h.lv[0].L = lat_of(h.lv[0].g);
-    h.lv[0].A = *A0;
-    for (int q = 1; q < h.nl; ++q) {
-        MgLevel &c = h.lv[q];
-        c.L = lat_of(c.g);
-        c.A.n_rows = plan->n_rows[q];
-        c.A.nnzb = plan->nnzb[q];
-        c.A.nf = nf;
-        c.A.mask_words = mw;
-    }
-}
-
-// Numeric phase: smoother blocks and fixed-DOF masks of every level, Galerkin
-// values of the coarse levels, dense inverse of the coarsest.  No host reads.
-template <int NF, typename VT>
-int mg_numeric(MgHier &h, cudaStream_t s) {
-    const int D = h.lv[0].g.dim;
-    {
-        const MgLevel &l0 = h.lv[0];
-        PtrsA a0 = make_ptrs(l0.A);
-        k_mg_smoother_setup<NF, VT><<<gw_count_launch(nblk(l0.A.n_rows, kThreads)), kThreads, 0, s>>>(a0, D, l0.Minv);
-        k_mg_fixed_mask<NF, VT><<<gw_count_launch(nblk(l0.A.n_rows, kThreads)), kThreads, 0, s>>>(a0, l0.fixed);
-        GW_LAUNCHED();
-    }
-    for (int l = 0; l + 1 < h.nl; ++l) {
-        MgLevel &f = h.lv[l], &c = h.lv[l + 1];
-        PtrsA fa = make_ptrs(f.A), ca = make_ptrs(c.A);
-        const int nb = c.A.nnzb;
-        if (D == 2) {
-            if (l == 0) k_mg_rap<2, NF, VT><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-            else k_mg_rap<2, NF, double><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-        } else {
-            if (l == 0) k_mg_rap<3, NF, VT><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-            else k_mg_rap<3, NF, double><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-        }
-        GW_LAUNCHED();
-        const int nrc = c.A.n_rows;
-        k_mg_fix_empty_rows<NF><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca);
-        k_mg_smoother_setup<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, D, c.Minv);
-        k_mg_fixed_mask<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, c.fixed);
-        GW_LAUNCHED();
-    }
-    const int l = h.nl - 1;
-    const MgLevel &lc = h.lv[l];
-    const int n = h.dn;
-    GW_CUDA(cudaMemsetAsync(h.dM, 0, 8 * (size_t)n * n, s));
-    PtrsA ac = make_ptrs(lc.A);
-    if (l == 0) k_mg_dense_build<NF, VT><<<gw_count_launch(nblk(lc.A.n_rows, kThreads)), kThreads, 0, s>>>(ac, h.dM, n);
-    else k_mg_dense_build<NF, double><<<gw_count_launch(nblk(lc.A.n_rows, kThreads)), kThreads, 0, s>>>(ac, h.dM, n);
-    const size_t smem = 8 * (size_t)n * n;
-    GW_CUDA(cudaFuncSetAttribute(k_mg_dense_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 8 * kMgCoarseMax * kMgCoarseMax));
-    k_mg_dense_invert<<<gw_count_launch(1), 1024, smem, s>>>(h.dM, h.dInv, n);
-    GW_LAUNCHED();
-    return GW_OK;
-}
-
-template <int NF, typename VT>
-void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, double *xout, int zero, const int *skip,
-               cudaStream_t s) {
-    const MgLevel &v = h.lv[l];
-    PtrsA a = make_ptrs(v.A);
-    const int g = zero ? red_grid_elems(v.A.n_rows) : tune_rows_grid(v.A.n_rows);
-    const int tb = zero ? kThreads : tune_rows_block();
-    // algorithmic bytes: b, x_out, Minv; with a previous iterate also x_in and the matrix
-    const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
-    ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
-                 2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
-    if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
-    else k_mg_jacobi<NF, double><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
-}
-
-// One V-cycle on h.lv[0].b; returns the buffer that holds the result (the same
-// buffer on every call).
-template <int NF, typename VT>
-double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
-    const int last = h.nl - 1;
-    const int D = h.lv[0].g.dim;
-    double *cur[kMgMaxLevels], *oth[kMgMaxLevels];
-    for (int l = 0; l < last; ++l) {
-        const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
-        double *x = v.x, *y = v.x2;
-        if (mg_sweeps(l) == 2) {
-            // both zero-start sweeps in one launch, into the buffer the
-            // second separate sweep would have written
-            PtrsA a = make_ptrs(v.A);
-            const double vs = 8.0 * v.A.n_rows * NF;
-            const double mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
-            ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
-            if (l == 0)
-                k_mg_presmooth2<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
-                    a, v.Minv, v.b, y, kMgOmega, skip);
-            else
-                k_mg_presmooth2<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
-                    a, v.Minv, v.b, y, kMgOmega, skip);
-            double *t = x; x = y; y = t;
-        } else {
-            mg_jacobi<NF, VT>(h, l, v.b, nullptr, x, 1, skip, s);
-            for (int it = 1; it < mg_sweeps(l); ++it) {
-                mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
-                double *t = x; x = y; y = t;
-            }
-        }
-        PtrsA a = make_ptrs(v.A), ca = make_ptrs(c.A);
-        const double vs = 8.0 * v.A.n_rows * NF;
-        {
-        ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4));
-        if (l == 0) k_mg_residual<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
-        else k_mg_residual<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
-        }
-        ProfScope ps(PC_MG_TRANSFER, s, vs + 8.0 * c.A.n_rows * NF);
-        if (D == 2) k_mg_restrict<2, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, v.r, c.b, skip);
-        else k_mg_restrict<3, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, v.r, c.b, skip);
-        cur[l] = x;
-        oth[l] = y;
-    }
-    const MgLevel &lc = h.lv[last];
-    k_mg_dense_apply<<<gw_count_launch(nblk((int64_t)h.dn * 32, kThreads)), kThreads, 0, s>>>(h.dInv, lc.b, lc.x, h.dn, skip);
-    cur[last] = lc.x;
-    for (int l = last - 1; l >= 0; --l) {
-        const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
-        PtrsA a = make_ptrs(v.A), ca = make_ptrs(c.A);
-        double *x = cur[l], *y = oth[l];
-        {
-        ProfScope ps(PC_MG_TRANSFER, s, 16.0 * v.A.n_rows * NF + 8.0 * c.A.n_rows * NF);
-        if (D == 2) k_mg_prolong<2, NF><<<gw_count_launch(nblk(v.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, cur[l + 1], x, skip);
-        else k_mg_prolong<3, NF><<<gw_count_launch(nblk(v.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, cur[l + 1], x, skip);
-        }
-        for (int it = 0; it < mg_sweeps(l); ++it) {
-            mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
-            double *t = x; x = y; y = t;
-        }
-        cur[l] = x;
-    }
-    return cur[0];
-}
-
-// One Arnoldi step with its V-cycle is ~40 small kernels.  Issuing them one by
-// one costs more host time than the GPU spends running them, so the step is
-// captured once as a CUDA graph and replayed.  Every kernel argument of the
-// step is fixed by the key below (matrix, vectors, workspace, plan), so one
-// instantiated graph serves all Newton iterations of a load step.  The graphs
-// are held in a small cache (least recently used entry replaced).
-struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps;
-    int n_grid[3];
-    int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
-    gw_bsr_t A;
-    const void *ws;
-    const double *b;
-    double *x, *z;
-};
-struct MgGraphEntry {
-    bool valid;
-    MgGraphKey key;
-    cudaGraphExec_t exec;
-    int64_t nodes;
-    uint64_t stamp;
-};
-constexpr int kMgGraphCache = 8;
-int g_gm_last_iters = 0;  // iterations of the previous multigrid GMRES solve (first-chunk hint)
-MgGraphEntry g_mg_graphs[kMgGraphCache];
-uint64_t g_mg_graph_clock = 0;
-cudaStream_t g_capture_stream[64] = {};
-
-int capture_stream(cudaStream_t *out) {
-    int dev = 0;
-    GW_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return GW_EINVAL;
-    if (!g_capture_stream[dev]) GW_CUDA(cudaStreamCreateWithFlags(&g_capture_stream[dev], cudaStreamNonBlocking));
-    *out = g_capture_stream[dev];
-    return GW_OK;
-}
-
-template <int NF, typename VT>
-void mg_arnoldi_step(const MgHier &h, const PtrsA &a, const GmresVecs &G, double *Z, int gr, int gv, size_t n,
-                     const int *skip, cudaStream_t s) {
-    k_gm_spmv_keep<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, Z);
-    k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0);
-    k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0);
-    k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1);
-    k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1);
-    k_gm_next_flex<<<gw_count_launch(gv), kThreads, 0, s>>>(n, G, 0, h.lv[0].b);
-    mg_vcycle<NF, VT>(h, skip, s);
-}
-
-// Returns the cached (or newly captured) graph of one Arnoldi step.
-template <int NF, typename VT>
-int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, const GmresVecs &G, double *Z, void *ws,
-                  int restart, int gr, int gv, size_t n, const int *skip, cudaGraphExec_t *exec, int64_t *nodes) {
-    MgGraphKey k;
-    memset(&k, 0, sizeof(k));
-    GW_CUDA(cudaGetDevice(&k.device));
-    k.nf = NF; k.vt_bytes = sizeof(VT); k.restart = restart; k.nl = h.nl; k.dn = h.dn; k.dim = grid.dim;
-    k.row_warps = g_tune[GW_TUNE_ROW_WARPS];
-    for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
-    for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
-    k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;
-    int victim = -1;
-    for (int e = 0; e < kMgGraphCache; ++e) {
-        MgGraphEntry &ent = g_mg_graphs[e];
-        if (ent.valid && memcmp(&ent.key, &k, sizeof(k)) == 0) {
-            ent.stamp = ++g_mg_graph_clock;
-            *exec = ent.exec;
-            *nodes = ent.nodes;
-            return GW_OK;
-        }
-        // an empty slot first, else the least recently used one
-        if (victim < 0 || (g_mg_graphs[victim].valid && (!ent.valid || ent.stamp < g_mg_graphs[victim].stamp)))
-            victim = e;
-    }
-    cudaStream_t cs;
-    int rc = capture_stream(&cs);
-    if (rc) return rc;
-    PtrsA a = make_ptrs(*A);
-    const int64_t before = g_launches;
-    GW_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    mg_arnoldi_step<NF, VT>(h, a, G, Z, gr, gv, n, skip, cs);
-    cudaGraph_t graph;
-    const cudaError_t ce = cudaStreamEndCapture(cs, &graph);
-    const int64_t count = g_launches - before;
-    g_launches = before;  // counted when the graph is replayed
-    GW_CUDA(ce);
-    cudaGraphExec_t ge;
-    const cudaError_t ie = cudaGraphInstantiate(&ge, graph, 0);
-    cudaGraphDestroy(graph);
-    GW_CUDA(ie);
-    MgGraphEntry &slot = g_mg_graphs[victim];
-    if (slot.valid) GW_CUDA(cudaGraphExecDestroy(slot.exec));
-    slot.valid = true;
-    slot.key = k;
-    slot.exec = ge;
-    slot.nodes = count;
-    slot.stamp = ++g_mg_graph_clock;
-    *exec = ge;
-    *nodes = count;
-    return GW_OK;
-}
-
-template <int NF, typename VT>
-int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_in, const double *b, double *x,
-             double rtol, int max_iter, int restart, void *ws, int64_t ws_bytes, int *iters, double *relres,
-             cudaStream_t s) {
-    const int nr = A->n_rows;
-    if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
-    const int64_t n = (int64_t)nr * NF;
-    Bump bp{(char *)ws, 0};
-    MgHier h;
-    FlexVecs fv;
-    mg_carve_hier(bp, h, *grid, nr, NF);
-    mg_carve_flex(bp, fv, n, restart);
-    if (bp.used > ws_bytes) {
-        snprintf(g_msg, sizeof(g_msg), "multigrid GMRES: workspace of %lld bytes, %lld needed", (long long)ws_bytes,
-                 (long long)bp.used);
-        return GW_EINVAL;
-    }
-    int rc;
-    {
-        ProfScope ps(PC_MG_SETUP, s, (double)A->nnzb * (NF * NF * sizeof(VT) + 4));
-        gw_mg_plan_t local;
-        if (plan_in) {
-            if (plan_in->workspace != ws || plan_in->nf != NF || plan_in->fine_n_rows != nr ||
-                plan_in->fine_nnzb != A->nnzb || plan_in->levels < 1 || plan_in->levels > h.nl ||
-                plan_in->dense_n != plan_in->n_rows[plan_in->levels - 1] * NF || plan_in->dense_n > kMgCoarseMax) {
-                snprintf(g_msg, sizeof(g_msg), "multigrid GMRES: the plan was built for another workspace or pattern");
-                return GW_EINVAL;
-            }
-            mg_apply_plan(h, A, plan_in, NF);
-        } else {
-            rc = mg_pattern<NF>(h, A, &local, s);
-            if (rc) return rc;
-        }
-        // lag: the previous solve's coarse operators, smoothers and dense
-        // inverse are still in the workspace; GMRES itself applies A
-        rc = (plan_in && plan_in->lag) ? GW_OK : mg_numeric<NF, VT>(h, s);
-    }
-    if (rc) return rc;
-    PtrsA a = make_ptrs(*A);
-    GmresVecs G;
-    G.V = fv.V; G.w = fv.w; G.partials = fv.partials; G.sc = fv.sc; G.Minv = nullptr;
-    G.x = x; G.b = b; G.n = (size_t)n;
-    G.z = nullptr;
-    const size_t head = offsetof(GScalars, H);
-    GW_CUDA(cudaMemsetAsync(G.sc, 0, head, s));
-    struct { int max_iter, restart; } lim = {max_iter, restart};
-    GW_CUDA(cudaMemcpyAsync(&G.sc->max_iter, &lim, sizeof(lim), cudaMemcpyHostToDevice, s));
-    const int gr = red_grid_rows(nr), gv = red_grid_elems(n);
-    const int *skip = &G.sc->cycle_done;
-    GScalars hs;
-    memset(&hs, 0, head);
-    int first = 1;
-    for (int cycle = 0; cycle < 1000000; ++cycle) {
-        k_gm_residual<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, first, rtol);
-        k_gm_next_flex<<<gw_count_launch(gv), kThreads, 0, s>>>((size_t)n, G, 1, h.lv[0].b);
-        GW_LAUNCHED();
-        G.z = mg_vcycle<NF, VT>(h, skip, s);
-        GW_LAUNCHED();
-        first = 0;
-        GW_CUDA(cudaMemcpyAsync(&hs, G.sc, head, cudaMemcpyDeviceToHost, s));
-        GW_CUDA(cudaStreamSynchronize(s));
-        if (hs.done) break;
-        // Arnoldi steps queued before the next host check: the previous
-        // solve's iteration count to start with (Newton solves of a step look
-        // alike), then the iterations left at the observed convergence rate.
-        // Steps queued past convergence still launch their (early-exiting)
-        // kernels, so the estimate trims them without adding host reads.
-        int chunk = g_gm_last_iters > 0 ? std::min(std::max(g_gm_last_iters, 2), 16) : 4;
-        int kk = 0;
-        const double spmv_bytes = (double)A->nnzb * (NF * NF * sizeof(VT) + 4) + 4.0 * (nr + 1) + 24.0 * n;
-        cudaGraphExec_t step_graph = nullptr;
-        int64_t step_nodes = 0;
-        if (!g_prof_on) {  // timed runs launch kernel by kernel, bracketed by events
-            rc = mg_step_graph<NF, VT>(h, *grid, A, G, fv.Z, ws, restart, gr, gv, (size_t)n, skip, &step_graph,
-                                       &step_nodes);
-            if (rc) return rc;
-        }
-        for (;;) {
-            for (int it = 0; it < chunk; ++it, ++kk) {
-                if (step_graph) {
-                    GW_CUDA(cudaGraphLaunch(step_graph, s));
-                    g_launches += step_nodes;
-                    continue;
-                }
-                const double vb = 8.0 * n * (kk + 2);
-                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv_keep<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, fv.Z); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_NEXT, s, 8.0 * n * 3); k_gm_next_flex<<<gw_count_launch(gv), kThreads, 0, s>>>((size_t)n, G, 0, h.lv[0].b); }
-                mg_vcycle<NF, VT>(h, skip, s);
-            }
-            GW_LAUNCHED();
-            GW_CUDA(cudaMemcpyAsync(&hs, G.sc, head, cudaMemcpyDeviceToHost, s));
-            GW_CUDA(cudaStreamSynchronize(s));
-            if (hs.cycle_done) break;
-            int next = chunk < 16 ? chunk * 2 : 16;
-            if (hs.k > 0 && hs.beta > 0.0 && hs.resid > 0.0 && hs.resid < hs.beta && hs.tol > 0.0) {
-                const double rate = ::pow(hs.resid / hs.beta, 1.0 / hs.k);
-                if (rate < 1.0) {
-                    const double left = ::ceil(::log(hs.tol / hs.resid) / ::log(rate));
-                    next = left < 1.0 ? 1 : (left > 16.0 ? 16 : (int)left);
-                }
-            }
-            chunk = next;
-        }
-        if (hs.status) break;
-        k_gm_solve_y<<<gw_count_launch(1), 32, 0, s>>>(G.sc);
-        k_gm_update_x_flex<<<gw_count_launch(gv), kThreads, 0, s>>>((size_t)n, G, fv.Z);
-        GW_LAUNCHED();
-    }
-    *iters = hs.iters;
-    *relres = (hs.bnorm > 0.0) ? hs.resid / hs.bnorm : 0.0;
-    g_gm_last_iters = hs.iters;
-    if (hs.status == ST_NAN) return GW_ENAN;
-    if (hs.resid > hs.tol) return GW_ENOCONV;
-    return GW_OK;
-}
-
-template <typename VT>
-int gmres_mg_nf(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan, const double *b, double *x,
-                double rtol, int max_iter, int restart, void *ws, int64_t ws_bytes, int *iters, double *relres,
-                cudaStream_t s) {
-    switch (A->nf) {
-        case 1: return gmres_mg<1, VT>(grid, A, plan, b, x, rtol, max_iter, restart, ws, ws_bytes, iters, relres, s);
-        case 2: return gmres_mg<2, VT>(grid, A, plan, b, x, rtol, max_iter, restart, ws, ws_bytes, iters, relres, s);
-        case 3: return gmres_mg<3, VT>(grid, A, plan, b, x, rtol, max_iter, restart, ws, ws_bytes, iters, relres, s);
-        case 4: return gmres_mg<4, VT>(grid, A, plan, b, x, rtol, max_iter, restart, ws, ws_bytes, iters, relres, s);
-        default: return GW_EINVAL;
-    }
-}
-
-int mg_check_args(const gw_grid_t *grid, const gw_bsr_t *A) {
-    GW_REQUIRE(grid->dim == 2 || grid->dim == 3);
-    GW_REQUIRE(A->mask_words == (grid->dim == 2 ? 1 : 4));
-    GW_REQUIRE(A->n_rows <= grid->n_nodes);
-    GW_REQUIRE(A->nf >= 1 && A->nf <= 4);
-    return GW_OK;
-}
-}  // namespace
-
-extern "C" int64_t gw_gmres_mg_workspace_bytes(const gw_grid_t *grid, int32_t n_rows, int32_t nf, int32_t restart) {
-    if (!grid || restart < 1 || restart > kGmresMaxRestart || nf < 1 || nf > 4 || n_rows < 0) return -1;
-    return mg_ws_bytes(*grid, n_rows, nf, restart);
-}
-
-extern "C" int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *workspace, int64_t workspace_bytes,
-                                gw_mg_plan_t *plan_host, void *stream) {
-    GW_REQUIRE(grid && A && workspace && plan_host);
-    int rc = mg_check_args(grid, A);
-    if (rc) return rc;
-    Bump bp{(char *)workspace, 0};
-    MgHier h;
-    mg_carve_hier(bp, h, *grid, A->n_rows, A->nf);
-    if (bp.used > workspace_bytes) {
-        snprintf(g_msg, sizeof(g_msg), "multigrid plan: workspace of %lld bytes, %lld needed",
-                 (long long)workspace_bytes, (long long)bp.used);
-        return GW_EINVAL;
-    }
-    cudaStream_t s = S(stream);
-    switch (A->nf) {
-        case 1: rc = mg_pattern<1>(h, A, plan_host, s); break;
-        case 2: rc = mg_pattern<2>(h, A, plan_host, s); break;
-        case 3: rc = mg_pattern<3>(h, A, plan_host, s); break;
-        default: rc = mg_pattern<4>(h, A, plan_host, s); break;
-    }
-    if (rc) return rc;
-    plan_host->workspace = workspace;
-    return GW_OK;
-}
-
-extern "C" int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec,
-                                     const gw_mg_plan_t *plan_host, const double *b, double *x, double rtol,
-                                     int32_t max_iter, int32_t restart, void *workspace, int64_t workspace_bytes,
-                                     int32_t *iters_host, double *relres_host, void *stream) {
-    GW_REQUIRE(grid && A && b && x && workspace && iters_host && relres_host && max_iter > 0);
-    GW_REQUIRE(vec_ok(A, b, x));
-    GW_REQUIRE(restart >= 1 && restart <= kGmresMaxRestart);
-    int rc = mg_check_args(grid, A);
-    if (rc) return rc;
-    int it = 0;
-    double rr = 0.0;
-    rc = (prec == GW_PREC_F64)
-             ? gmres_mg_nf<double>(grid, A, plan_host, b, x, rtol, max_iter, restart, workspace, workspace_bytes, &it,
-                                   &rr, S(stream))
-             : gmres_mg_nf<float>(grid, A, plan_host, b, x, rtol, max_iter, restart, workspace, workspace_bytes, &it,
-                                  &rr, S(stream));
-    *iters_host = it;
-    *relres_host = rr;
-    return rc;
-}
-
-extern "C" int64_t gw_krylov_workspace_bytes(int32_t n_rows, int32_t nf, int32_t prec) {
-    (void)prec;
-    return krylov_ws_bytes(n_rows, nf);
-}
-
-extern "C" int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond, const double *b,
-                                   double *x, double rtol, int32_t max_iter, void *workspace, int32_t *iters_host,
-                                   double *relres_host, void *stream) {
-    GW_REQUIRE(A && b && x && workspace && iters_host && relres_host && max_iter > 0);
-    GW_REQUIRE(vec_ok(A, b, x));
-    int it = 0;
-    double rr = 0.0;
-    int rc = (prec == GW_PREC_F64)
-                 ? krylov_nf<double>(A, method, precond, b, x, rtol, max_iter, workspace, &it, &rr, S(stream))
-                 : krylov_nf<float>(A, method, precond, b, x, rtol, max_iter, workspace, &it, &rr, S(stream));
-    *iters_host = it;
-    *relres_host = rr;
-    return rc;
-}
-
-// ==================================================================== Krylov without a caller workspace
-// For callers that cannot allocate device memory themselves: a host whose own
-// memory manager owns the device heap, or a code path where calling cudaMalloc
-// is not allowed.  The scratch the BiCGSTAB / CG driver needs lives in one
-// file-scope device array, sized for at most kStaticKrylovMaxUnknowns unknowns
-// (n_rows * nf); every GPU that loads the library holds it (about 12.6 MB)
-// until the process exits.
-namespace {
-constexpr int64_t kStaticKrylovMaxUnknowns = 131072;
-constexpr int64_t align256c(int64_t b) { return (b + 255) & ~(int64_t)255; }
-// krylov_ws_bytes at the limit, for the largest block size (nf = 4)
-constexpr int64_t kStaticKrylovBytes = 8 * align256c(8 * kStaticKrylovMaxUnknowns) +
-                                       align256c(8 * kStaticKrylovMaxUnknowns * 4) +
-                                       align256c(8 * (int64_t)kRedBlocks * 4) + align256c(sizeof(KScalars));
-static __device__ __align__(256) unsigned char g_krylov_scratch[kStaticKrylovBytes];
-
-constexpr int kMaxStaticDevices = 64;
-void *g_krylov_scratch_addr[kMaxStaticDevices] = {};
-
-// Device address of g_krylov_scratch on the current device.  The name is only a
-// host-side stand-in, so the address is looked up once per device, with that
-// device current, and cached.
-int static_krylov_scratch(void **out) {
-    int dev = 0;
-    GW_CUDA(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxStaticDevices) {
-        snprintf(g_msg, sizeof(g_msg), "gw_bsr_krylov_solve_static: device ordinal %d above %d", dev,
-                 kMaxStaticDevices - 1);
-        return GW_EINVAL;
-    }
-    void *p = __atomic_load_n(&g_krylov_scratch_addr[dev], __ATOMIC_ACQUIRE);
-    if (!p) {
-        GW_CUDA(cudaGetSymbolAddress(&p, g_krylov_scratch));
-        __atomic_store_n(&g_krylov_scratch_addr[dev], p, __ATOMIC_RELEASE);
-    }
-    *out = p;
-    return GW_OK;
-}
-}  // namespace
-
-extern "C" int64_t gw_krylov_static_max_unknowns(void) { return kStaticKrylovMaxUnknowns; }
-
-extern "C" int gw_bsr_krylov_solve_static(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t precond,
-                                          const double *b, double *x, double rtol, int32_t max_iter,
-                                          int32_t *iters_host, double *relres_host, void *stream) {
-    GW_REQUIRE(A && b && x && iters_host && relres_host && max_iter > 0);
-    GW_REQUIRE(vec_ok(A, b, x));
-    const int64_t unknowns = (int64_t)A->n_rows * A->nf;
-    if (A->n_rows < 0 || A->nf < 1 || A->nf > 4 || unknowns > kStaticKrylovMaxUnknowns ||
-        krylov_ws_bytes(A->n_rows, A->nf) > kStaticKrylovBytes) {
-        snprintf(g_msg, sizeof(g_msg),
-                 "gw_bsr_krylov_solve_static: %lld unknowns (n_rows %d x nf %d) exceed the static scratch limit of "
-                 "%lld unknowns; use gw_bsr_krylov_solve with a caller workspace",
-                 (long long)unknowns, A->n_rows, A->nf, (long long)kStaticKrylovMaxUnknowns);
-        return GW_EINVAL;
-    }
-    void *ws = nullptr;
-    const int rs = static_krylov_scratch(&ws);
-    if (rs != GW_OK) return rs;
-    // the driver clears the scalar block (reduction ticket, flags) on every call
-    // and writes every vector before reading it, so the contents a previous call
-    // left in the scratch are never used
-    int it = 0;
-    double rr = 0.0;
-    int rc = (prec == GW_PREC_F64)
-                 ? krylov_nf<double>(A, method, precond, b, x, rtol, max_iter, ws, &it, &rr, S(stream))
-                 : krylov_nf<float>(A, method, precond, b, x, rtol, max_iter, ws, &it, &rr, S(stream));
-    *iters_host = it;
-    *relres_host = rr;
-    return rc;
-}
-
-namespace {
-template <typename VT>
-int spmv_any(const gw_bsr_t *A, const double *x, double *y, bool trans, cudaStream_t s) {
-    PtrsA a = make_ptrs(*A);
-    const int g = red_grid_rows(A->n_rows);
-    if (A->n_rows == 0) return GW_OK;
-    if (trans) GW_CUDA(cudaMemsetAsync(y, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
-#define GW_SPMV_CASE(NF_)                                                  \
-    case NF_:                                                              \
-        if (trans) k_spmv_t<NF_, VT><<<gw_count_launch(g), kThreads, 0, s>>>(a, x, y);      \
-        else k_spmv<NF_, VT><<<gw_count_launch(g), kThreads, 0, s>>>(a, x, y);              \
-        break;
-    switch (A->nf) {
-        GW_SPMV_CASE(1) GW_SPMV_CASE(2) GW_SPMV_CASE(3) GW_SPMV_CASE(4)
-        default: return GW_EINVAL;
-    }
-#undef GW_SPMV_CASE
-    GW_LAUNCHED();
-    return GW_OK;
-}
-}  // namespace
-
-extern "C" int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream) {
-    GW_REQUIRE(A && x && y);
-    GW_REQUIRE(vec_ok(A, x, y));
-    return prec == GW_PREC_F64 ? spmv_any<double>(A, x, y, false, S(stream)) : spmv_any<float>(A, x, y, false, S(stream));
-}
-
-extern "C" int gw_bsr_spmv_t(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream) {
-    GW_REQUIRE(A && x && y);
-    return prec == GW_PREC_F64 ? spmv_any<double>(A, x, y, true, S(stream)) : spmv_any<float>(A, x, y, true, S(stream));
-}
 
 extern "C" int gw_norm2(const double *v, int32_t n, double *norm_dev, void *workspace, void *stream) {
     GW_REQUIRE(v && norm_dev && workspace);
@@ -1453,94 +289,7 @@ extern "C" int gw_return_map(const gw_material_t *mat, int32_t n, const double *
     return GW_OK;
 }
 
-// ==================================================================== adjoint (2D solid)
-namespace {
-AdjState make_adj(const gw_adjoint_t &a) {
-    AdjState s;
-    s.x = a.x; s.lp = a.lp; s.F = a.F; s.b = a.b; s.E = a.E;
-    return s;
-}
-}  // namespace
 
-extern "C" int gw_bsr_transpose(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, void *AT_vals, void *stream) {
-    GW_REQUIRE(grid && A && AT_vals);
-    if (A->n_rows == 0) return GW_OK;
-    PtrsA a = make_ptrs(*A);
-    cudaStream_t s = S(stream);
-    const size_t vb = (prec == GW_PREC_F64 ? 8 : 4) * (size_t)A->nnzb * A->nf * A->nf;
-    GW_CUDA(cudaMemsetAsync(AT_vals, 0, vb, s));
-    const int b = nblk(A->n_rows, kThreads / 32);
-    if (grid->dim == 2) {
-        if (prec == GW_PREC_F64) k_bsr_transpose<2, double><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
-        else k_bsr_transpose<2, float><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
-    } else {
-        if (prec == GW_PREC_F64) k_bsr_transpose<3, double><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (double *)AT_vals);
-        else k_bsr_transpose<3, float><<<gw_count_launch(b), kThreads, 0, s>>>(*grid, a, (float *)AT_vals);
-    }
-    GW_LAUNCHED();
-    return GW_OK;
-}
-
-extern "C" int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
-                              const gw_particles_t *pt, const double *u_new, const double *u_old,
-                              const uint8_t *free_mask, const gw_bsr_t *A, const gw_adjoint_t *seed_in,
-                              gw_adjoint_t *q_out, double *ubar_rows, void *stream) {
-    GW_REQUIRE(grid && mat && st && pt && u_new && u_old && free_mask && A && seed_in && q_out && ubar_rows);
-    if (grid->kind != GW_KIND_SOLID2D) return GW_EMODEL;
-    if (mat->model == GW_MODEL_NORSAND) return GW_EMODEL;
-    cudaStream_t s = S(stream);
-    GW_CUDA(cudaMemsetAsync(ubar_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
-    if (pt->n == 0) return GW_OK;
-    LaunchConst c = make_lc(grid, mat, st);
-    c.mc.tip_tangent = 0.0;  // exact derivatives of the converged state
-    ProfScope ps(PC_ADJ_G2P, s, (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 18 + 23 + 2 * 9 * 2));
-    const int ab = g_tune[GW_TUNE_ADJOINT_BLOCK];
-    const dim3 grd(gw_count_launch(nblk(pt->n, ab))), blk(ab);
-    const PtrsP pp = make_ptrs(*pt);
-    const PtrsA pa = make_ptrs(*A);
-    const AdjState si = make_adj(*seed_in), qo = make_adj(*q_out);
-    switch (mat->model) {  // one instantiation per material: see solid2d_dual
-        case GW_MODEL_HENCKY: k_adjoint_g2p<GW_MODEL_HENCKY><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
-        case GW_MODEL_J2: k_adjoint_g2p<GW_MODEL_J2><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
-        case GW_MODEL_DP: k_adjoint_g2p<GW_MODEL_DP><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
-        case GW_MODEL_NEOHOOKEAN: k_adjoint_g2p<GW_MODEL_NEOHOOKEAN><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
-        case GW_MODEL_LINEAR: k_adjoint_g2p<GW_MODEL_LINEAR><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
-        default: k_adjoint_g2p<-1><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
-    }
-    GW_LAUNCHED();
-    return GW_OK;
-}
-
-extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
-                                   const gw_particles_t *pt, const double *u_new, const double *u_old,
-                                   const uint8_t *free_mask, const gw_bsr_t *A, const double *lambda_rows,
-                                   gw_adjoint_t *q_out, void *stream) {
-    GW_REQUIRE(grid && mat && st && pt && u_new && u_old && free_mask && A && lambda_rows && q_out);
-    if (grid->kind != GW_KIND_SOLID2D) return GW_EMODEL;
-    if (mat->model == GW_MODEL_NORSAND) return GW_EMODEL;
-    if (pt->n == 0) return GW_OK;
-    LaunchConst c = make_lc(grid, mat, st);
-    c.mc.tip_tangent = 0.0;  // exact derivatives of the converged residual
-    ProfScope ps(PC_ADJ_RES, S(stream), (double)pt->n * 8.0 * (2 + 2 + 9 + 9 + 1 + 23 * 2 + 2 * 9 * 2 + 9 * 2));
-    const int ab = g_tune[GW_TUNE_ADJOINT_BLOCK];
-    const dim3 grd(gw_count_launch(nblk(pt->n, ab))), blk(ab);
-    const PtrsP pp = make_ptrs(*pt);
-    const PtrsA pa = make_ptrs(*A);
-    const AdjState qo = make_adj(*q_out);
-    cudaStream_t s = S(stream);
-    switch (mat->model) {  // one instantiation per material: see solid2d_dual
-        case GW_MODEL_HENCKY: k_adjoint_residual<GW_MODEL_HENCKY><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
-        case GW_MODEL_J2: k_adjoint_residual<GW_MODEL_J2><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
-        case GW_MODEL_DP: k_adjoint_residual<GW_MODEL_DP><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
-        case GW_MODEL_NEOHOOKEAN: k_adjoint_residual<GW_MODEL_NEOHOOKEAN><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
-        case GW_MODEL_LINEAR: k_adjoint_residual<GW_MODEL_LINEAR><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
-        default: k_adjoint_residual<-1><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
-    }
-    GW_LAUNCHED();
-    return GW_OK;
-}
-
-// ==================================================================== kernel timing
 extern "C" int64_t gw_launch_count(void) { return g_launches; }
 
 extern "C" int gw_tune_set(int32_t knob, int32_t value) {

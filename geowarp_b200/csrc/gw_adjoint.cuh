@@ -15,6 +15,7 @@
 #include "gw_step_kernels.cuh"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 constexpr int kAdjLanes = 19;
 typedef Dual<kAdjLanes, double> AD;
@@ -333,6 +334,7 @@ __global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__
         const uint8_t fm = free_mask[id];
         if (!fm) continue;
         const int row = A.node2row[id];
+        if (!in_range(row, A.n_rows, GS_ADJOINT)) continue;
         for (int l = 0; l < 2; ++l) {
             if (!((fm >> l) & 1)) continue;
             const double v = Hb[0][l] * o.G[b][0] + Hb[1][l] * o.G[b][1] + o.W[b] * xb_eff[l];
@@ -373,6 +375,7 @@ __global__ void k_adjoint_residual(LaunchConst c, PtrsP p, const double *__restr
         const uint8_t fm = free_mask[id];
         if (!fm) continue;
         const int row = A.node2row[id];
+        if (!in_range(row, A.n_rows, GS_ADJOINT)) continue;
         for (int f = 0; f < 2; ++f)
             if ((fm >> f) & 1) s += o.r[a][f] * lambda_rows[(size_t)row * 2 + f];
     }
@@ -402,11 +405,19 @@ __global__ void k_bsr_transpose(gw_grid_t g, PtrsA A, VT *__restrict__ AT) {
     const VT *vals = (const VT *)A.vals;
     for (int j = A.row_ptr[r] + lane; j < A.row_ptr[r + 1]; j += 32) {
         const int cr = A.cols[j];
+        if (!in_range(cr, A.n_rows, GS_TRANSPOSE)) continue;
         const int cnode = A.row2node[cr];
+        if (!in_range(cnode, g.n_nodes, GS_TRANSPOSE)) continue;
         int off[3] = {0, 0, 0}, q = cnode;
-        for (int k = 0; k < D; ++k) { off[k] = ic[k] - q % (g.n_grid[k] + 1); q /= (g.n_grid[k] + 1); }
+        bool ok = true;
+        for (int k = 0; k < D; ++k) {
+            off[k] = ic[k] - q % (g.n_grid[k] + 1);
+            q /= (g.n_grid[k] + 1);
+            ok = ok && in_range(off[k] + 2, 5, GS_TRANSPOSE);
+        }
+        if (!ok) continue;
         const int slot = stencil_slot(A.stencil, A.mw, cnode, offset_bit<D>(off));
-        if (slot < 0) continue;
+        if (slot < 0 || !in_range((long long)A.row_ptr[cr] + slot, A.nnzb, GS_TRANSPOSE)) continue;
         const VT *src = vals + (size_t)j * nf * nf;
         VT *dst = AT + ((size_t)A.row_ptr[cr] + slot) * nf * nf;
         for (int f = 0; f < nf; ++f)
@@ -414,4 +425,5 @@ __global__ void k_bsr_transpose(gw_grid_t g, PtrsA A, VT *__restrict__ AT) {
     }
 }
 
+}  // namespace
 }  // namespace gw

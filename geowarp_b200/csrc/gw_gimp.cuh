@@ -8,6 +8,7 @@
 #include "gw_math.cuh"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 struct Axis {
     int lower;    // lower-corner cell (node index of slot 0)
@@ -77,4 +78,5 @@ struct Shape {
     }
 };
 
+}  // namespace
 }  // namespace gw

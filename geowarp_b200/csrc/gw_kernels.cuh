@@ -1,13 +1,48 @@
-// Shared kernel-side definitions.  The library is one translation unit
-// (gw_abi.cu includes every kernel header), so device globals live here.
+// Shared kernel-side definitions: particle / matrix pointer bundles, the
+// stencil-slot lookup, the device status word and the index guards.
 #pragma once
 #include "gw_particle.cuh"
 
 namespace gw {
 
+// Device globals shared by every translation unit of the library (relocatable
+// device code): defined in the one that sets GW_DEFINE_DEVICE_GLOBALS.
+#ifdef GW_DEFINE_DEVICE_GLOBALS
+#define GW_DEVICE_GLOBAL __device__
+#else
+#define GW_DEVICE_GLOBAL extern __device__
+#endif
 // Device status word: bit 0 range error, bit 1 non-finite value, bit 2 Krylov breakdown.
-__device__ int g_status;
+GW_DEVICE_GLOBAL int g_status;
+// first failed index guard (site, value): see in_range below
+GW_DEVICE_GLOBAL int g_guard_site;
+GW_DEVICE_GLOBAL long long g_guard_value;
+
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
+
 constexpr int ST_RANGE = 1, ST_NAN = 2, ST_BREAKDOWN = 4;
+
+// Index guards.  Every index the solver kernels compute from a row map, a
+// column array, a stencil or a Krylov counter is checked against the extent
+// of the array it addresses before the access.  A failed check skips the
+// access, sets ST_RANGE and records the first failing site and its value
+// (gw_guard_read), so a corrupted pattern surfaces as GW_ERANGE on the host
+// instead of as a memory fault.
+enum GuardSite {
+    GS_NONE = 0, GS_ROW_MV, GS_COARSE_FLAGS, GS_COARSE_STENCIL, GS_PATTERN_FILL, GS_RAP_COARSE, GS_RAP_FINE,
+    GS_SMOOTHER, GS_RESTRICT, GS_PROLONG, GS_DENSE, GS_KRYLOV_K, GS_TRANSPOSE, GS_ASSEMBLE, GS_ADJOINT,
+    GS_BLOCKROW, GS_FIXED, GS_PRESMOOTH, GS_COUNT
+};
+__device__ __noinline__ void guard_fail(int site, long long v) {
+    atomicOr(&g_status, ST_RANGE);
+    if (atomicCAS(&g_guard_site, 0, site) == 0) g_guard_value = v;
+}
+// true when 0 <= i < n; otherwise records the failure
+__device__ __forceinline__ bool in_range(long long i, long long n, int site) {
+    if ((unsigned long long)i < (unsigned long long)n) return true;
+    guard_fail(site, i);
+    return false;
+}
 
 struct PtrsP {  // particle pointers as seen by kernels
     int n;
@@ -59,4 +94,5 @@ __device__ __forceinline__ int offset_bit(const int off[3]) {
     return b;
 }
 
+}  // namespace
 }  // namespace gw

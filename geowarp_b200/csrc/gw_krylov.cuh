@@ -11,6 +11,7 @@
 #include "gw_kernels.cuh"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 constexpr int kRedBlocks = 148 * 8;  // grid size of reduction kernels (multiple of the B200 SM count)
 
@@ -137,6 +138,7 @@ __device__ __forceinline__ void row_mv(const PtrsA &A, int r, const double *__re
     const VT *vals = (const VT *)A.vals;
     for (int j = s + lane; j < e; j += 32) {
         const int col = A.cols[j];
+        if (!in_range(col, A.n_rows, GS_ROW_MV)) continue;
         double xv[NF], bv[NF * NF];
         load_vec<NF>(x + (size_t)col * NF, xv);
         load_block<NF, VT>(vals + (size_t)j * NF * NF, bv);
@@ -175,6 +177,7 @@ __global__ void k_spmv_t(PtrsA A, const double *__restrict__ x, double *__restri
         for (int f = 0; f < NF; ++f) xr[f] = x[(size_t)r * NF + f];
         for (int j = A.row_ptr[r] + lane; j < A.row_ptr[r + 1]; j += 32) {
             const int col = A.cols[j];
+            if (!in_range(col, A.n_rows, GS_ROW_MV)) continue;
             const VT *blk = vals + (size_t)j * NF * NF;
 #pragma unroll
             for (int g = 0; g < NF; ++g) {
@@ -536,9 +539,11 @@ __global__ void k_apply_increment(int n_rows, int nf, const int *__restrict__ ro
     for (int f = 0; f < nf; ++f) u[(size_t)node * nf + f] += delta[(size_t)r * nf + f];
 }
 
+}  // namespace
 }  // namespace gw
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 // ---------------------------------------------------------------- restarted GMRES(m)
 // Right-preconditioned GMRES with classical Gram-Schmidt and one
@@ -617,6 +622,7 @@ template <int NF>
 __global__ void k_gm_next(int n_rows, GmresVecs G, int start) {
     if (G.sc->cycle_done) return;
     const int k = G.sc->k;
+    if (!in_range(k, G.sc->restart + 1, GS_KRYLOV_K)) return;
     const double ih = 1.0 / (start ? G.sc->beta : G.sc->wnorm);
     double *vn = G.V + (size_t)k * G.n;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += gridDim.x * blockDim.x) {
@@ -647,6 +653,7 @@ __global__ void k_gm_spmv(PtrsA A, GmresVecs G) {
 __global__ void k_gm_dots(GmresVecs G, int pass) {
     if (G.sc->cycle_done) return;
     const int k = G.sc->k;
+    if (!in_range(k, G.sc->restart, GS_KRYLOV_K)) return;  // uniform over the grid: no block takes the ticket
     const size_t n = G.n;
     __shared__ double sh[kGmresMaxRestart + 1];
     __shared__ bool last;
@@ -693,6 +700,7 @@ __global__ void k_gm_update(GmresVecs G, int pass) {
     if (G.sc->cycle_done) return;
     GScalars *sc = G.sc;
     const int k = sc->k;
+    if (!in_range(k, sc->restart, GS_KRYLOV_K)) return;  // uniform over the grid
     const size_t n = G.n;
     __shared__ double coef[kGmresMaxRestart + 1];
     for (int i = threadIdx.x; i <= k; i += blockDim.x) coef[i] = pass == 0 ? sc->H[i][k] : sc->h2[i];
@@ -737,6 +745,7 @@ __global__ void k_gm_update(GmresVecs G, int pass) {
 __global__ void k_gm_solve_y(GScalars *sc) {
     if (threadIdx.x != 0 || blockIdx.x != 0 || sc->done) return;
     const int k = sc->k;
+    if (!in_range(k, sc->restart + 1, GS_KRYLOV_K)) return;
     for (int i = k - 1; i >= 0; --i) {
         double s = sc->g[i];
         for (int q = i + 1; q < k; ++q) s -= sc->H[i][q] * sc->y[q];
@@ -750,6 +759,7 @@ __global__ void k_gm_update_x(int n_rows, GmresVecs G) {
     const GScalars *sc = G.sc;
     if (sc->done) return;
     const int k = sc->k;
+    if (!in_range(k, sc->restart + 1, GS_KRYLOV_K)) return;
     for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n_rows; r += gridDim.x * blockDim.x) {
         double u[NF], z[NF];
 #pragma unroll
@@ -764,4 +774,5 @@ __global__ void k_gm_update_x(int n_rows, GmresVecs G) {
     }
 }
 
+}  // namespace
 }  // namespace gw

@@ -9,6 +9,7 @@
 #define GW_HD __host__ __device__ __forceinline__
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 // ---------------------------------------------------------------- scalar helpers
 GW_HD double val(double x) { return x; }
@@ -266,4 +267,5 @@ GW_HD void eig_sym3(const R Ain[3][3], R lam[3], R V[3][3]) {
     lam[2] = A[2][2];
 }
 
+}  // namespace
 }  // namespace gw

@@ -32,6 +32,7 @@
 #include "gw_krylov.cuh"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 constexpr int kMgMaxLevels = GW_MG_MAX_LEVELS;
 // unknowns of the coarsest (dense) level: its n x n FP64 matrix (204,800 bytes
@@ -56,6 +57,7 @@ __device__ __forceinline__ void lat_coords(const Lat &L, int id, int c[3]) {
     c[2] = t / L.n[1];
 }
 __device__ __forceinline__ int lat_id(const Lat &L, const int c[3]) { return c[0] + L.n[0] * (c[1] + L.n[1] * c[2]); }
+__host__ __device__ inline int lat_size(const Lat &L) { return L.n[0] * L.n[1] * L.n[2]; }
 
 // 1D prolongation weight of fine coordinate f below coarse coordinate C
 __device__ __forceinline__ double p_weight(int f, int C) {
@@ -92,8 +94,10 @@ __global__ void k_mg_fixed_mask(PtrsA A, uint8_t *__restrict__ fixed) {
 __global__ void k_mg_coarse_flags(Lat Lf, PtrsA Af, Lat Lc, uint8_t *__restrict__ cflag) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= Af.n_rows) return;
+    const int node = Af.row2node[r];
+    if (!in_range(node, lat_size(Lf), GS_COARSE_FLAGS)) return;
     int c[3];
-    lat_coords(Lf, Af.row2node[r], c);
+    lat_coords(Lf, node, c);
     int lo[3], cnt[3];
     for (int k = 0; k < 3; ++k) {
         lo[k] = c[k] >> 1;
@@ -103,7 +107,8 @@ __global__ void k_mg_coarse_flags(Lat Lf, PtrsA Af, Lat Lc, uint8_t *__restrict_
         for (int b = 0; b < cnt[1]; ++b)
             for (int d = 0; d < cnt[2]; ++d) {
                 const int C[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
-                cflag[lat_id(Lc, C)] = 1;
+                const int id = lat_id(Lc, C);
+                if (in_range(id, lat_size(Lc), GS_COARSE_FLAGS)) cflag[id] = 1;
             }
 }
 
@@ -114,6 +119,7 @@ __global__ void k_mg_coarse_stencil(Lat Lf, PtrsA Af, Lat Lc, int nc_rows, const
     const int R = blockIdx.x * blockDim.x + threadIdx.x;
     if (R >= nc_rows) return;
     const int I = c_row2node[R];
+    if (!in_range(I, lat_size(Lc), GS_COARSE_STENCIL)) return;
     int C[3];
     lat_coords(Lc, I, C);
     uint32_t mask[4] = {0u, 0u, 0u, 0u};
@@ -146,6 +152,9 @@ __global__ void k_mg_coarse_stencil(Lat Lf, PtrsA Af, Lat Lc, int nc_rows, const
                             for (int b = 0; b < cnt[1]; ++b)
                                 for (int d = 0; d < cnt[2]; ++d) {
                                     const int off[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
+                                    bool ok = true;
+                                    for (int k = 0; k < D; ++k) ok = ok && in_range(off[k] + 2, 5, GS_COARSE_STENCIL);
+                                    if (!ok) continue;
                                     const int ob = offset_bit<D>(off);
                                     mask[ob >> 5] |= 1u << (ob & 31);
                                 }
@@ -161,10 +170,11 @@ __global__ void k_mg_coarse_stencil(Lat Lf, PtrsA Af, Lat Lc, int nc_rows, const
 }
 
 // block -> row map of a block-CSR (for one-thread-per-block kernels)
-__global__ void k_mg_blockrow(const int *__restrict__ row_ptr, int n_rows, int *__restrict__ blockrow) {
+__global__ void k_mg_blockrow(const int *__restrict__ row_ptr, int n_rows, int nnzb, int *__restrict__ blockrow) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
-    for (int j = row_ptr[r]; j < row_ptr[r + 1]; ++j) blockrow[j] = r;
+    for (int j = row_ptr[r]; j < row_ptr[r + 1]; ++j)
+        if (in_range(j, nnzb, GS_BLOCKROW)) blockrow[j] = r;
 }
 
 // ---------------------------------------------------------------- Galerkin product
@@ -175,8 +185,17 @@ __global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, L
                          const int *__restrict__ c_blockrow) {
     const int jb = blockIdx.x * blockDim.x + threadIdx.x;
     if (jb >= Ac.nnzb) return;
-    const int R = c_blockrow[jb];
-    const int I = Ac.row2node[R], J = Ac.row2node[Ac.cols[jb]];
+    const int R = c_blockrow[jb], Rc = Ac.cols[jb];
+    double *out = (double *)Ac.vals + (size_t)jb * NF * NF;
+    if (!in_range(R, Ac.n_rows, GS_RAP_COARSE) || !in_range(Rc, Ac.n_rows, GS_RAP_COARSE)) {
+        for (int q = 0; q < NF * NF; ++q) out[q] = 0.0;
+        return;
+    }
+    const int I = Ac.row2node[R], J = Ac.row2node[Rc];
+    if (!in_range(I, lat_size(Lc), GS_RAP_COARSE) || !in_range(J, lat_size(Lc), GS_RAP_COARSE)) {
+        for (int q = 0; q < NF * NF; ++q) out[q] = 0.0;
+        return;
+    }
     int CI[3], CJ[3];
     lat_coords(Lc, I, CI);
     lat_coords(Lc, J, CJ);
@@ -195,7 +214,7 @@ __global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, L
                 if (!in) continue;
                 const int i = lat_id(Lf, ci);
                 const int fr = Af.node2row[i];
-                if (fr < 0) continue;
+                if (fr < 0 || !in_range(fr, Af.n_rows, GS_RAP_FINE)) continue;
                 double wi = 1.0;
                 for (int k = 0; k < D; ++k) wi *= p_weight(ci[k], CI[k]);
                 const uint8_t fi = ffixed[fr];
@@ -213,11 +232,13 @@ __global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, L
                             const int slot = stencil_slot(Af.stencil, Af.mw, i, offset_bit<D>(off));
                             if (slot < 0) continue;
                             const int fc = Af.node2row[lat_id(Lf, cj)];
-                            if (fc < 0) continue;
+                            if (fc < 0 || !in_range(fc, Af.n_rows, GS_RAP_FINE)) continue;
+                            const long long fb = (long long)Af.row_ptr[fr] + slot;
+                            if (!in_range(fb, Af.nnzb, GS_RAP_FINE)) continue;
                             double wj = 1.0;
                             for (int k = 0; k < D; ++k) wj *= p_weight(cj[k], CJ[k]);
                             const uint8_t fj = ffixed[fc];
-                            const VT *blk = vals + ((size_t)Af.row_ptr[fr] + slot) * NF * NF;
+                            const VT *blk = vals + (size_t)fb * NF * NF;
                             const double w = wi * wj;
 #pragma unroll
                             for (int f = 0; f < NF; ++f) {
@@ -228,7 +249,6 @@ __global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, L
                             }
                         }
             }
-    double *out = (double *)Ac.vals + (size_t)jb * NF * NF;
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
@@ -290,11 +310,14 @@ __global__ void k_mg_smoother_setup(PtrsA A, int D, double *__restrict__ Minv) {
                 m &= m - 1u;
                 const int k = A.row_ptr[r] + s++;
                 if (bit == center) continue;
+                if (!in_range(k, A.nnzb, GS_SMOOTHER)) continue;
                 const int col = A.cols[k];
+                if (!in_range(col, A.n_rows, GS_SMOOTHER)) continue;
                 const int nj = A.row2node[col];
                 const int tj = stencil_slot(A.stencil, A.mw, nj, top - bit);
                 const int dj = stencil_slot(A.stencil, A.mw, nj, center);
                 if (tj < 0 || dj < 0) continue;
+                if (!in_range((long long)A.row_ptr[col] + (tj > dj ? tj : dj), A.nnzb, GS_SMOOTHER)) continue;
                 const VT *b_ij = vals + (size_t)k * NF * NF;
                 const VT *b_ji = vals + ((size_t)A.row_ptr[col] + tj) * NF * NF;
                 const VT *b_jj = vals + ((size_t)A.row_ptr[col] + dj) * NF * NF;
@@ -363,6 +386,7 @@ __global__ void k_mg_presmooth2(PtrsA A, const double *__restrict__ Minv, const 
         const int s0 = A.row_ptr[r], e0 = A.row_ptr[r + 1];
         for (int j = s0 + lane; j < e0; j += 32) {
             const int col = A.cols[j];
+            if (!in_range(col, A.n_rows, GS_PRESMOOTH)) continue;
             double t[NF], z[NF], bv[NF * NF];
             load_vec<NF>(b + (size_t)col * NF, t);
             load_block<NF, VT>(vals + (size_t)j * NF * NF, bv);
@@ -414,8 +438,10 @@ __global__ void k_mg_restrict(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffix
     if (skip && *skip) return;
     const int R = blockIdx.x * blockDim.x + threadIdx.x;
     if (R >= Ac.n_rows) return;
+    const int I = Ac.row2node[R];
+    if (!in_range(I, lat_size(Lc), GS_RESTRICT)) return;
     int C[3];
-    lat_coords(Lc, Ac.row2node[R], C);
+    lat_coords(Lc, I, C);
     double acc[NF];
 #pragma unroll
     for (int f = 0; f < NF; ++f) acc[f] = 0.0;
@@ -427,7 +453,7 @@ __global__ void k_mg_restrict(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffix
                 for (int k = 0; k < D; ++k) in = in && ci[k] >= 0 && ci[k] < Lf.n[k];
                 if (!in) continue;
                 const int fr = Af.node2row[lat_id(Lf, ci)];
-                if (fr < 0) continue;
+                if (fr < 0 || !in_range(fr, Af.n_rows, GS_RESTRICT)) continue;
                 double w = 1.0;
                 for (int k = 0; k < D; ++k) w *= p_weight(ci[k], C[k]);
                 const uint8_t fx = ffixed[fr];
@@ -446,8 +472,10 @@ __global__ void k_mg_prolong(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixe
     if (skip && *skip) return;
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= Af.n_rows) return;
+    const int node = Af.row2node[r];
+    if (!in_range(node, lat_size(Lf), GS_PROLONG)) return;
     int c[3];
-    lat_coords(Lf, Af.row2node[r], c);
+    lat_coords(Lf, node, c);
     int lo[3], cnt[3];
     for (int k = 0; k < 3; ++k) {
         lo[k] = c[k] >> 1;
@@ -460,8 +488,10 @@ __global__ void k_mg_prolong(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixe
         for (int b = 0; b < cnt[1]; ++b)
             for (int d = 0; d < cnt[2]; ++d) {
                 const int C[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
-                const int R = Ac.node2row[lat_id(Lc, C)];
-                if (R < 0) continue;
+                const int cid = lat_id(Lc, C);
+                if (!in_range(cid, lat_size(Lc), GS_PROLONG)) continue;
+                const int R = Ac.node2row[cid];
+                if (R < 0 || !in_range(R, Ac.n_rows, GS_PROLONG)) continue;
                 double w = 1.0;
                 for (int k = 0; k < D; ++k) w *= p_weight(c[k], C[k]);
 #pragma unroll
@@ -482,6 +512,7 @@ __global__ void k_mg_dense_build(PtrsA A, double *__restrict__ M, int n) {
     const VT *vals = (const VT *)A.vals;
     for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1]; ++j) {
         const int c = A.cols[j];
+        if (!in_range(c, A.n_rows, GS_DENSE) || !in_range((long long)(r + 1) * NF, (long long)n + 1, GS_DENSE)) continue;
         for (int f = 0; f < NF; ++f)
             for (int g = 0; g < NF; ++g)
                 M[(size_t)(r * NF + f) * n + c * NF + g] = (double)vals[(size_t)j * NF * NF + f * NF + g];
@@ -592,6 +623,7 @@ __global__ void k_mg_dense_apply(const double *__restrict__ Inv, const double *_
 __global__ void k_gm_next_flex(size_t n, GmresVecs G, int start, double *__restrict__ mg_b) {
     if (G.sc->cycle_done) return;
     const int k = G.sc->k;
+    if (!in_range(k, G.sc->restart + 1, GS_KRYLOV_K)) return;  // V holds restart + 1 vectors
     const double ih = 1.0 / (start ? G.sc->beta : G.sc->wnorm);
     double *vn = G.V + (size_t)k * G.n;
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
@@ -605,6 +637,7 @@ __global__ void k_gm_next_flex(size_t n, GmresVecs G, int start, double *__restr
 template <int NF, typename VT>
 __global__ void k_gm_spmv_keep(PtrsA A, GmresVecs G, double *__restrict__ Z) {
     if (G.sc->cycle_done) return;
+    if (!in_range(G.sc->k, G.sc->restart, GS_KRYLOV_K)) return;  // Z holds restart vectors
     double *zk = Z + (size_t)G.sc->k * G.n;
     const int nw = gridDim.x * (blockDim.x >> 5);
     for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
@@ -624,6 +657,7 @@ __global__ void k_gm_update_x_flex(size_t n, GmresVecs G, const double *__restri
     const GScalars *sc = G.sc;
     if (sc->done) return;
     const int k = sc->k;
+    if (!in_range(k, sc->restart + 1, GS_KRYLOV_K)) return;
     for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
         double s = 0.0;
         for (int i = 0; i < k; ++i) s += sc->y[i] * Z[(size_t)i * n + q];
@@ -631,4 +665,5 @@ __global__ void k_gm_update_x_flex(size_t n, GmresVecs G, const double *__restri
     }
 }
 
+}  // namespace
 }  // namespace gw

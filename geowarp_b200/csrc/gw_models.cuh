@@ -11,6 +11,7 @@
 #include "../../include/geowarp_b200.h"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 // Per-material constants, precomputed on the host side of each launch.
 struct MatConst {
@@ -337,4 +338,5 @@ GW_HD void principal_model(const MatConst &c, R lam, R mu, const R etr_v[3], R e
     }
 }
 
+}  // namespace
 }  // namespace gw

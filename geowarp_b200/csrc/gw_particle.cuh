@@ -21,6 +21,7 @@
 #include "gw_models.cuh"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 template <int KIND> struct KindTraits;
 template <> struct KindTraits<GW_KIND_SOLID2D> { static const int D = 2, NF = 2, NS = 9; static const bool UP = false; };
@@ -493,4 +494,5 @@ GW_HD void residual_rows(const LaunchConst &c, const PState<KIND> &s, const PEva
     }
 }
 
+}  // namespace
 }  // namespace gw

@@ -4,6 +4,7 @@
 #include "gw_kernels.cuh"
 
 namespace gw {
+namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 constexpr int kThreads = 256;
 constexpr int kSortTile = 2048;
@@ -44,6 +45,12 @@ __global__ void k_scan_block(const int *__restrict__ in, int *__restrict__ out, 
     const int incl = x + (w > 0 ? ws[w - 1] : 0);
     if (i < n) out[i] = incl - v;
     if (threadIdx.x == 1023 && sums) sums[blockIdx.x] = incl;
+}
+
+// *out = *a + *b (one thread): the total of an exclusive scan from its last
+// element and the last input flag
+__global__ void k_add2(const int *a, const int *b, int *out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *out = *a + *b;
 }
 
 __global__ void k_scan_add(int *__restrict__ out, int n, const int *__restrict__ offs) {
@@ -281,7 +288,9 @@ __global__ void k_pattern_fill(gw_grid_t g, PtrsA A, int *__restrict__ cols) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.n_rows) return;
     const int node = A.row2node[r];
+    if (!in_range(node, g.n_nodes, GS_PATTERN_FILL)) return;
     int pos = A.row_ptr[r];
+    const int end = A.row_ptr[r + 1];
     for (int w = 0; w < A.mw; ++w) {
         uint32_t m = A.stencil[(size_t)node * A.mw + w];
         while (m) {
@@ -294,7 +303,9 @@ __global__ void k_pattern_fill(gw_grid_t g, PtrsA A, int *__restrict__ cols) {
                 bit /= 5;
                 jid += o * node_stride(g, k);
             }
-            cols[pos++] = A.node2row[jid];
+            if (!in_range(pos, end, GS_PATTERN_FILL)) return;
+            const int col = in_range(jid, g.n_nodes, GS_PATTERN_FILL) ? A.node2row[jid] : 0;
+            cols[pos++] = in_range(col, A.n_rows, GS_PATTERN_FILL) ? col : 0;
         }
     }
 }
@@ -347,6 +358,7 @@ __global__ void __launch_bounds__(kThreads) k_assemble(LaunchConst c, PtrsP p, c
         const uint8_t fm = free_mask[id];
         if (!fm) continue;
         const int row = A.node2row[id];
+        if (!in_range(row, A.n_rows, GS_ASSEMBLE)) continue;
         double r[NF];
         residual_rows<KIND>(c, s, ev, a, fext, ftr, V0, r);
         for (int f = 0; f < NF; ++f)
@@ -392,11 +404,14 @@ __global__ void __launch_bounds__(kThreads) k_assemble(LaunchConst c, PtrsP p, c
             const uint8_t fma = free_mask[ida];
             if (!fma) continue;
             const int row = A.node2row[ida];
+            if (!in_range(row, A.n_rows, GS_ASSEMBLE)) continue;
             int off[3] = {0, 0, 0};
             for (int k = 0; k < D; ++k) off[k] = s.sh.idx(b, k) - s.sh.idx(a, k);
             const int slot = stencil_slot(A.stencil, A.mw, ida, offset_bit<D>(off));
             if (slot < 0) { atomicOr(&g_status, ST_RANGE); continue; }
-            VT *blk = vals + ((size_t)A.row_ptr[row] + slot) * NF * NF;
+            const long long jb = (long long)A.row_ptr[row] + slot;
+            if (!in_range(jb, A.nnzb, GS_ASSEMBLE)) continue;
+            VT *blk = vals + (size_t)jb * NF * NF;
             const double Wa_ = s.sh.W(a), Waa = s.sh.Wavg(a);
             double Ga[D];
             for (int k = 0; k < D; ++k) Ga[k] = s.sh.G(a, k);
@@ -560,4 +575,5 @@ __global__ void k_return_map(MatConst mc, double lam, double mu, int n, const do
     }
 }
 
+}  // namespace
 }  // namespace gw

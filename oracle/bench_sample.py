@@ -223,3 +223,59 @@ def oracle_bar_sample(n_steps=50, max_steps=50, budget_s=15.0, threads=1):
             f"iterations per step, complex-step tangents and SciPy spsolve), NumPy oracle with {threads} host "
             f"thread(s) for the tangent passes")
     return sec, n, desc
+
+
+def batch_block_oracle(nx, ny, logE, dx=0.05, PPD=2, rho=2000.0, gravity=9.81, nu=0.3, n_iter=20, tol=1e-6):
+    """One block of the batched inverse analysis on its own grid (two empty
+    cells around it): Hencky elastic with the block's per-particle Young's
+    modulus exp(logE), self-weight ramped over the load steps, rollers on its
+    side node columns and a fixed base row (the boundary of every packed block)."""
+    pad = 2
+    n_grid_x, n_grid_y = nx + 2 * pad, ny + 2 * pad
+    sx, sy = pad * dx, pad * dx
+    ex, ey = sx + nx * dx, sy + ny * dx
+    x = init_particles_rectangle_2d(sx, sy, ex, ey, dx, n_grid_x, n_grid_y, PPD, nx * ny * PPD * PPD)
+    mat = dict(youngs_modulus=1e7, poisson_ratio=nu, material_name="Hencky elasticity")
+    load = dict(gravity_mag=gravity, traction_value_x=0.0, traction_value_y=0.0, point_load_value_x=0.0,
+                point_load_value_y=0.0)
+    grid = dict(n_grid=(n_grid_x, n_grid_y), h=(dx, dx), h_nodes=(dx, dx), domain_min=(sx, sy), domain_max=(ex, ey))
+    o = OracleEngine("solid2d", grid, x, (dx / PPD) ** 2, rho, PPD, mat, load, lp0=dx / PPD / 2.0 - 1e-6,
+                     n_iter=n_iter, tol=tol, E_field=np.exp(np.asarray(logE, dtype=np.float64)))
+    nn = (n_grid_x + 1) * (n_grid_y + 1)
+    ix = np.tile(np.arange(n_grid_x + 1), n_grid_y + 1)
+    iy = np.repeat(np.arange(n_grid_y + 1), n_grid_x + 1)
+    col = ((ix == pad) | (ix == pad + nx)) & (iy >= pad) & (iy <= pad + ny)
+    base = (iy == pad) & (ix >= pad) & (ix <= pad + nx)
+    o.boundary[(col | base).nonzero()[0]] = True
+    o.boundary[base.nonzero()[0] + nn] = True
+    return o
+
+
+def oracle_batch_sample(sizes, logE, n_steps, budget_s=20.0, threads=1, max_blocks=None):
+    """Block load steps per second of the batched inverse analysis in the
+    oracle: load step 0 (P2G, Newton to the tolerance with complex-step
+    tangents and a SciPy sparse direct solve, G2P) of whole blocks, taken in
+    the batch's order until budget_s is spent (at least one block).  The
+    blocks are independent, so blocks / seconds is the workload's own unit.
+    Returns (block load steps per second, blocks run, description)."""
+    offs = np.cumsum([0] + [a * b * 4 for a, b in sizes])
+    t0 = time.perf_counter()
+    n = 0
+    its = []
+    parts = 0
+    while n < len(sizes) and (max_blocks is None or n < max_blocks):
+        nx, ny = sizes[n]
+        o = batch_block_oracle(nx, ny, logE[offs[n]:offs[n + 1]])
+        o.threads = threads
+        o.advance_one_step(0, n_steps)
+        its.append(o.iters[-1] if o.iters else 0)
+        parts += o.N
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    sec = time.perf_counter() - t0
+    desc = (f"load step 0 of {n_steps} (forward: P2G, {np.mean(its):.1f} Newton iterations with complex-step "
+            f"tangents and SciPy spsolve, G2P) of blocks 0..{n - 1} of the batch ({parts} particles, sizes "
+            f"{', '.join(f'{a}x{b}' for a, b in sizes[:n])}), NumPy oracle with {threads} host thread(s) for the "
+            f"tangent passes; the CPU path has no adjoint")
+    return n / sec, n, desc
