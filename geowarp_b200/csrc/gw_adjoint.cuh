@@ -7,23 +7,37 @@
 //   q_bar = d(out)/dq^T out_bar + R_q^T lambda,   K^T lambda = d(out)/du^T out_bar,
 // where out = (x_new, lp_new, F_new, b_new) are the G2P outputs
 // (mpm/mpm_utils.py:1351-1419, mpm/gimp.py:428-462) and K = -dR/du the
-// converged Jacobian.  Both VJPs come from one forward-mode pass per particle
-// with 19 dual lanes through the same formulas as the forward kernels:
-//   lanes 0-1 x, 2-3 lp, 4-8 F_old (00,01,10,11,22), 9-12 b_old (00,01=10,11,22),
+// converged Jacobian.  Both VJPs are directional derivatives of one scalar,
+// s = sum(output . weight) -- the G2P outputs weighted by their seeds, or the
+// residual rows weighted by lambda -- with respect to 19 particle inputs:
+//   inputs 0-1 x, 2-3 lp, 4-8 F_old (00,01,10,11,22), 9-12 b_old (00,01=10,11,22),
 //   13 E, 14-17 H (00,01,10,11), 18 ubar_y (penalty footing).
+// They come from forward-mode dual passes through the same formulas as the
+// forward kernels, chunked: each pass carries kAdjChunk dual lanes (a window
+// of the inputs) and contracts every output with its weight as soon as it is
+// formed, so no per-row Jacobian is kept and a pass fits in registers.  The
+// 19 inputs take four passes (the residual adjoint, which needs inputs 0-13
+// only, takes three).
 #pragma once
 #include "gw_step_kernels.cuh"
 
 namespace gw {
 namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
-constexpr int kAdjLanes = 19;
-typedef Dual<kAdjLanes, double> AD;
+constexpr int kAdjInputs = 19;
+constexpr int kAdjChunk = 3;
+constexpr int kAdjLanes = kAdjChunk;  // dual lanes per pass
+typedef Dual<kAdjChunk, double> AD;
 constexpr int LX = 0, LLP = 2, LF = 4, LB = 9, LE = 13, LH = 14, LU = 18;
 
-GW_HD AD seed(double v, int lane) {
+// adds val to the lane of input `input` when it falls in this pass's window
+GW_HD void set_lane(AD &v, int input, int off, double val = 1.0) {
+    const int l = input - off;
+    if (l >= 0 && l < kAdjChunk) v.d[l] += val;
+}
+GW_HD AD seed(double v, int input, int off) {
     AD r(v);
-    if (lane >= 0) r.d[lane] = 1.0;
+    set_lane(r, input, off);
     return r;
 }
 
@@ -90,36 +104,43 @@ GW_HD void spectral_assemble(const double V[3][3], const double lamb[3], const A
     }
 }
 
+// Weights of the contracted outputs: lambda per slot and field for the
+// residual rows (zero on fixed DOFs), and / or the seeds of the G2P outputs.
+struct DualWeights {
+    const double (*r)[2];           // [9][2] or null
+    const double *x, *lp, *F, *b;   // G2P seeds ([2], [2], [9], [9]) or null
+};
+
 struct SolidDual {
-    AD r[9][2];        // residual rows per slot
-    AD F_new[3][3], b_new[3][3];
-    AD x_new[2], lp_new[2];
+    AD s;               // sum(output . weight) with this pass's lanes
     int nid[9];
     double W[9], G[9][2];
     int lower[2], span[2];
     double xnew_dx[2];  // d lp_new_k / d x_new_k (clip branch: 0, +1 or -1)
 };
 
-// Forward pass of one 2D solid particle in dual arithmetic.  du: nodal
-// increments of the 9 slots (u_new - u_old), values only.  MODEL is the
-// material (GW_MODEL_*) fixed at compile time, so an instantiation carries
-// only its own constitutive code (the return maps in 19-lane duals dominate
-// the stack frame); MODEL < 0 reads it from c at run time.
+// Forward pass of one 2D solid particle in dual arithmetic, lanes for inputs
+// off .. off + kAdjChunk - 1.  du: nodal increments of the 9 slots (u_new -
+// u_old), values only.  MODEL is the material (GW_MODEL_*) fixed at compile
+// time, so an instantiation carries only its own constitutive code; MODEL < 0
+// reads it from c at run time.
 template <int MODEL>
 GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lpv, const double *Fo_v,
-                             const double *bo_v, double Ev, const double fext[2], const double du[9][2], bool want_g2p,
-                             SolidDual &o) {
+                        const double *bo_v, double Ev, const double fext[2], const double du[9][2], int off,
+                        const DualWeights &wt, SolidDual &o) {
     const gw_grid_t &g = c.g;
-    AD x[2] = {seed(xv[0], LX), seed(xv[1], LX + 1)};
-    AD lp[2] = {seed(lpv[0], LLP), seed(lpv[1], LLP + 1)};
+    const bool want_g2p = wt.x != nullptr;
+    o.s = AD(0.0);
+    AD x[2] = {seed(xv[0], LX, off), seed(xv[1], LX + 1, off)};
+    AD lp[2] = {seed(lpv[0], LLP, off), seed(lpv[1], LLP + 1, off)};
     AD Fo[3][3], bo[3][3];
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) { Fo[i][j] = AD(Fo_v[i * 3 + j]); bo[i][j] = AD(bo_v[i * 3 + j]); }
-    Fo[0][0].d[LF] = 1.0; Fo[0][1].d[LF + 1] = 1.0; Fo[1][0].d[LF + 2] = 1.0; Fo[1][1].d[LF + 3] = 1.0;
-    Fo[2][2].d[LF + 4] = 1.0;
-    bo[0][0].d[LB] = 1.0; bo[0][1].d[LB + 1] = 1.0; bo[1][0].d[LB + 1] = 1.0; bo[1][1].d[LB + 2] = 1.0;
-    bo[2][2].d[LB + 3] = 1.0;
-    AD E = seed(Ev, LE);
+    set_lane(Fo[0][0], LF, off); set_lane(Fo[0][1], LF + 1, off); set_lane(Fo[1][0], LF + 2, off);
+    set_lane(Fo[1][1], LF + 3, off); set_lane(Fo[2][2], LF + 4, off);
+    set_lane(bo[0][0], LB, off); set_lane(bo[0][1], LB + 1, off); set_lane(bo[1][0], LB + 1, off);
+    set_lane(bo[1][1], LB + 2, off); set_lane(bo[2][2], LB + 3, off);
+    AD E = seed(Ev, LE, off);
     const double nu = c.nu;
     AD lam = E * (nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
     AD mu = E * (1.0 / (2.0 * (1.0 + nu)));
@@ -150,8 +171,9 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
         dx_p[0] += W[a] * du[a][0];
         dx_p[1] += W[a] * du[a][1];
     }
-    H[0][0].d[LH] += 1.0; H[0][1].d[LH + 1] += 1.0; H[1][0].d[LH + 2] += 1.0; H[1][1].d[LH + 3] += 1.0;
-    ubar.d[LU] += 1.0;
+    set_lane(H[0][0], LH, off); set_lane(H[0][1], LH + 1, off); set_lane(H[1][0], LH + 2, off);
+    set_lane(H[1][1], LH + 3, off);
+    set_lane(ubar, LU, off);
 
     // kinematics
     AD Finc[3][3];
@@ -161,10 +183,14 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
         for (int j = 0; j < 2; ++j) Finc[i][j] += H[i][j];
     AD det2 = Finc[0][0] * Finc[1][1] - Finc[0][1] * Finc[1][0];
     AD Finv[2][2] = {{Finc[1][1] / det2, -Finc[0][1] / det2}, {-Finc[1][0] / det2, Finc[0][0] / det2}};
-    matmul3(Finc, Fo, o.F_new);
-    AD J = det3(o.F_new);
+    AD F_new[3][3];
+    matmul3(Finc, Fo, F_new);
+    AD J = det3(F_new);
     AD btr[3][3];
     congruence3(Finc, bo, btr);
+    if (want_g2p)  // F_new is a G2P output
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) o.s += F_new[i][j] * wt.F[i * 3 + j];
 
     // stress (Kirchhoff) and b_new
     AD tau[3][3];
@@ -208,22 +234,28 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
             }
         }
         spectral_assemble(V, lamb, tA, limT, dbp, tau);
-        spectral_assemble(V, lamb, fB, limB, dbp, o.b_new);
+        if (want_g2p) {  // b_new is a G2P output
+            AD bn[3][3];
+            spectral_assemble(V, lamb, fB, limB, dbp, bn);
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) o.s += bn[i][j] * wt.b[i * 3 + j];
+        }
     } else {
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) o.b_new[i][j] = btr[i][j];
+        if (want_g2p)
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) o.s += btr[i][j] * wt.b[i * 3 + j];
         if (model == GW_MODEL_NEOHOOKEAN) {  // J sigma = mu (F F^T - I) + lam ln J I
             AD lnJ = glog(J);
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) {
-                    AD ff = o.F_new[i][0] * o.F_new[j][0] + o.F_new[i][1] * o.F_new[j][1] + o.F_new[i][2] * o.F_new[j][2];
+                    AD ff = F_new[i][0] * F_new[j][0] + F_new[i][1] * F_new[j][1] + F_new[i][2] * F_new[j][2];
                     tau[i][j] = mu * (ff - (i == j ? 1.0 : 0.0));
                     if (i == j) tau[i][j] += lam * lnJ;
                 }
         } else {  // linear: sigma = lam tr(eps) I + 2 mu eps, tau = J sigma
             AD eps[3][3];
             for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) eps[i][j] = (o.F_new[i][j] + o.F_new[j][i]) * 0.5 - (i == j ? 1.0 : 0.0);
+                for (int j = 0; j < 3; ++j) eps[i][j] = (F_new[i][j] + F_new[j][i]) * 0.5 - (i == j ? 1.0 : 0.0);
             AD tr = eps[0][0] + eps[1][1] + eps[2][2];
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) {
@@ -250,27 +282,29 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
             pen_on = true;
         }
     }
-    for (int a = 0; a < 9; ++a) {
-        AD wg[2];
-        for (int i = 0; i < 2; ++i) wg[i] = Finv[i][0] * G[a][0] + Finv[i][1] * G[a][1];
-        for (int j = 0; j < 2; ++j) {
-            AD v = -(wg[0] * tau[0][j] + wg[1] * tau[1][j]) * V0;
-            if (j == 1) v += W[a] * (c.st.p_rho * V0 * gv);
-            if (j == 1 && pen_on) v += pen * W[a];
-            v += W[a] * fext[j];
-            o.r[a][j] = v;
+    if (wt.r)
+        for (int a = 0; a < 9; ++a) {
+            if (wt.r[a][0] == 0.0 && wt.r[a][1] == 0.0) continue;
+            AD wg[2];
+            for (int i = 0; i < 2; ++i) wg[i] = Finv[i][0] * G[a][0] + Finv[i][1] * G[a][1];
+            for (int j = 0; j < 2; ++j) {
+                AD v = -(wg[0] * tau[0][j] + wg[1] * tau[1][j]) * V0;
+                if (j == 1) v += W[a] * (c.st.p_rho * V0 * gv);
+                if (j == 1 && pen_on) v += pen * W[a];
+                v += W[a] * fext[j];
+                o.s += v * wt.r[a][j];
+            }
         }
-    }
     if (!want_g2p) return;
     // G2P outputs: x_new = x + sum W du ; lp_new from F_new columns, clipped
-    for (int k = 0; k < 2; ++k) o.x_new[k] = x[k] + dx_p[k];
     for (int k = 0; k < 2; ++k) {
-        AD U = gsqrt(o.F_new[0][k] * o.F_new[0][k] + o.F_new[1][k] * o.F_new[1][k] + o.F_new[2][k] * o.F_new[2][k]);
+        const AD xn = x[k] + dx_p[k];
+        AD U = gsqrt(F_new[0][k] * F_new[0][k] + F_new[1][k] * F_new[1][k] + F_new[2][k] * F_new[2][k]);
         AD v = U * c.st.lp0;
         double dxd = 0.0;
-        if (o.x_new[k].v - v.v < c.g.domain_min[k]) { v = o.x_new[k] - (c.g.domain_min[k] + 1e-6); dxd = 1.0; }
-        if (o.x_new[k].v + v.v > c.g.domain_max[k]) { v = (c.g.domain_max[k] - 1e-6) - o.x_new[k]; dxd = -1.0; }
-        o.lp_new[k] = v;
+        if (xn.v - v.v < c.g.domain_min[k]) { v = xn - (c.g.domain_min[k] + 1e-6); dxd = 1.0; }
+        if (xn.v + v.v > c.g.domain_max[k]) { v = (c.g.domain_max[k] - 1e-6) - xn; dxd = -1.0; }
+        o.s += xn * wt.x[k] + v * wt.lp[k];
         o.xnew_dx[k] = dxd;
     }
 }
@@ -279,6 +313,37 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
 struct AdjState {  // per-particle adjoint arrays (user order)
     double *x, *lp, *F, *b, *E;  // [N*2], [N*2], [N*9], [N*9], [N]
 };
+
+// Nodal increments u_new - u_old of the particle's 9 slots (zero outside the grid).
+__device__ __forceinline__ void gather_du(const LaunchConst &c, const PtrsP &p, int pid, const double *__restrict__ u_new,
+                                          const double *__restrict__ u_old, double du[9][2]) {
+    int lower[2];
+    for (int k = 0; k < 2; ++k) lower[k] = cell_of(p.x[pid * 2 + k] - p.lp[pid * 2 + k], c.g.inv_h[k]);
+    for (int a = 0; a < 9; ++a) {
+        const int cx = lower[0] + a % 3, cy = lower[1] + a / 3;
+        const bool in = cx >= 0 && cx <= c.g.n_grid[0] && cy >= 0 && cy <= c.g.n_grid[1];
+        const int id = cx + cy * (c.g.n_grid[0] + 1);
+        for (int l = 0; l < 2; ++l) du[a][l] = in ? u_new[(size_t)id * 2 + l] - u_old[(size_t)id * 2 + l] : 0.0;
+    }
+}
+
+// Runs the chunked passes over inputs [0, n_inputs): q[i] = ds / d input_i.
+template <int MODEL>
+__device__ __forceinline__ void adjoint_passes(const LaunchConst &c, const PtrsP &p, int pid, const double du[9][2],
+                                               const DualWeights &wt, int n_inputs, double q[kAdjInputs],
+                                               SolidDual &o) {
+    const double E = p.E ? p.E[pid] : c.E0;
+    const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
+    const bool ext = p.ext_flag && p.ext_flag[pid];
+    const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
+    for (int off = 0; off < n_inputs; off += kAdjChunk) {
+        solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E,
+                            fext, du, off, wt, o);
+#pragma unroll
+        for (int l = 0; l < kAdjChunk; ++l)
+            if (off + l < kAdjInputs) q[off + l] = o.s.d[l];
+    }
+}
 
 // Adjoint G2P: seeds (x_new, lp_new, F_new, b_new) bars -> q_bar (written) and
 // the nodal adjoint u_bar (free DOFs of active rows, atomically accumulated).
@@ -289,45 +354,30 @@ __global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__
     const int pid = blockIdx.x * blockDim.x + threadIdx.x;
     if (pid >= p.n) return;
     double du[9][2];
-    {
-        int lower[2];
-        for (int k = 0; k < 2; ++k) lower[k] = cell_of(p.x[pid * 2 + k] - p.lp[pid * 2 + k], c.g.inv_h[k]);
-        for (int a = 0; a < 9; ++a) {
-            const int cx = lower[0] + a % 3, cy = lower[1] + a / 3;
-            const bool in = cx >= 0 && cx <= c.g.n_grid[0] && cy >= 0 && cy <= c.g.n_grid[1];
-            const int id = cx + cy * (c.g.n_grid[0] + 1);
-            for (int l = 0; l < 2; ++l) du[a][l] = in ? u_new[(size_t)id * 2 + l] - u_old[(size_t)id * 2 + l] : 0.0;
-        }
-    }
+    gather_du(c, p, pid, u_new, u_old, du);
+    DualWeights wt;
+    wt.r = nullptr;
+    wt.x = seed_in.x + pid * 2;
+    wt.lp = seed_in.lp + pid * 2;
+    wt.F = seed_in.F + (size_t)pid * 9;
+    wt.b = seed_in.b + (size_t)pid * 9;
+    double q[kAdjInputs];
     SolidDual o;
-    const double E = p.E ? p.E[pid] : c.E0;
-    const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
-    const bool ext = p.ext_flag && p.ext_flag[pid];
-    const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
-    solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
-                 true, o);
-    AD s(0.0);
+    adjoint_passes<MODEL>(c, p, pid, du, wt, kAdjInputs, q, o);
     double xb_eff[2];
-    for (int k = 0; k < 2; ++k) {
-        const double xb = seed_in.x[pid * 2 + k], lb = seed_in.lp[pid * 2 + k];
-        s += o.x_new[k] * xb + o.lp_new[k] * lb;
-        xb_eff[k] = xb + lb * o.xnew_dx[k];
-    }
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j)
-            s += o.F_new[i][j] * seed_in.F[(size_t)pid * 9 + i * 3 + j] + o.b_new[i][j] * seed_in.b[(size_t)pid * 9 + i * 3 + j];
+    for (int k = 0; k < 2; ++k) xb_eff[k] = wt.x[k] + wt.lp[k] * o.xnew_dx[k];
     // particle-input adjoints
-    q_out.x[pid * 2] = s.d[LX];
-    q_out.x[pid * 2 + 1] = s.d[LX + 1];
-    q_out.lp[pid * 2] = s.d[LLP];
-    q_out.lp[pid * 2 + 1] = s.d[LLP + 1];
+    q_out.x[pid * 2] = q[LX];
+    q_out.x[pid * 2 + 1] = q[LX + 1];
+    q_out.lp[pid * 2] = q[LLP];
+    q_out.lp[pid * 2 + 1] = q[LLP + 1];
     double *Fq = q_out.F + (size_t)pid * 9, *bq = q_out.b + (size_t)pid * 9;
     for (int k = 0; k < 9; ++k) { Fq[k] = 0.0; bq[k] = 0.0; }
-    Fq[0] = s.d[LF]; Fq[1] = s.d[LF + 1]; Fq[3] = s.d[LF + 2]; Fq[4] = s.d[LF + 3]; Fq[8] = s.d[LF + 4];
-    bq[0] = s.d[LB]; bq[1] = 0.5 * s.d[LB + 1]; bq[3] = 0.5 * s.d[LB + 1]; bq[4] = s.d[LB + 2]; bq[8] = s.d[LB + 3];
-    q_out.E[pid] = s.d[LE];
+    Fq[0] = q[LF]; Fq[1] = q[LF + 1]; Fq[3] = q[LF + 2]; Fq[4] = q[LF + 3]; Fq[8] = q[LF + 4];
+    bq[0] = q[LB]; bq[1] = 0.5 * q[LB + 1]; bq[3] = 0.5 * q[LB + 1]; bq[4] = q[LB + 2]; bq[8] = q[LB + 3];
+    q_out.E[pid] = q[LE];
     // nodal adjoint: H_bar_kl G_b,k on component l, plus W_b x_bar_eff
-    const double Hb[2][2] = {{s.d[LH], s.d[LH + 1]}, {s.d[LH + 2], s.d[LH + 3]}};
+    const double Hb[2][2] = {{q[LH], q[LH + 1]}, {q[LH + 2], q[LH + 3]}};
     for (int b = 0; b < 9; ++b) {
         const int id = o.nid[b];
         if (id < 0) continue;
@@ -351,42 +401,39 @@ __global__ void k_adjoint_residual(LaunchConst c, PtrsP p, const double *__restr
     const int pid = blockIdx.x * blockDim.x + threadIdx.x;
     if (pid >= p.n) return;
     double du[9][2];
+    gather_du(c, p, pid, u_new, u_old, du);
+    // lambda of the particle's slots (zero on fixed DOFs and outside the grid)
+    double lam_w[9][2];
     {
         int lower[2];
         for (int k = 0; k < 2; ++k) lower[k] = cell_of(p.x[pid * 2 + k] - p.lp[pid * 2 + k], c.g.inv_h[k]);
         for (int a = 0; a < 9; ++a) {
+            lam_w[a][0] = lam_w[a][1] = 0.0;
             const int cx = lower[0] + a % 3, cy = lower[1] + a / 3;
-            const bool in = cx >= 0 && cx <= c.g.n_grid[0] && cy >= 0 && cy <= c.g.n_grid[1];
+            if (cx < 0 || cx > c.g.n_grid[0] || cy < 0 || cy > c.g.n_grid[1]) continue;
             const int id = cx + cy * (c.g.n_grid[0] + 1);
-            for (int l = 0; l < 2; ++l) du[a][l] = in ? u_new[(size_t)id * 2 + l] - u_old[(size_t)id * 2 + l] : 0.0;
+            const uint8_t fm = free_mask[id];
+            if (!fm) continue;
+            const int row = A.node2row[id];
+            if (!in_range(row, A.n_rows, GS_ADJOINT)) continue;
+            for (int f = 0; f < 2; ++f)
+                if ((fm >> f) & 1) lam_w[a][f] = lambda_rows[(size_t)row * 2 + f];
         }
     }
+    DualWeights wt;
+    wt.r = lam_w;
+    wt.x = wt.lp = wt.F = wt.b = nullptr;
+    double q[kAdjInputs];
     SolidDual o;
-    const double E = p.E ? p.E[pid] : c.E0;
-    const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
-    const bool ext = p.ext_flag && p.ext_flag[pid];
-    const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
-    solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext, du,
-                 false, o);
-    AD s(0.0);
-    for (int a = 0; a < 9; ++a) {
-        const int id = o.nid[a];
-        if (id < 0) continue;
-        const uint8_t fm = free_mask[id];
-        if (!fm) continue;
-        const int row = A.node2row[id];
-        if (!in_range(row, A.n_rows, GS_ADJOINT)) continue;
-        for (int f = 0; f < 2; ++f)
-            if ((fm >> f) & 1) s += o.r[a][f] * lambda_rows[(size_t)row * 2 + f];
-    }
-    q_out.x[pid * 2] += s.d[LX];
-    q_out.x[pid * 2 + 1] += s.d[LX + 1];
-    q_out.lp[pid * 2] += s.d[LLP];
-    q_out.lp[pid * 2 + 1] += s.d[LLP + 1];
+    adjoint_passes<MODEL>(c, p, pid, du, wt, LE + 1, q, o);  // inputs x .. E
+    q_out.x[pid * 2] += q[LX];
+    q_out.x[pid * 2 + 1] += q[LX + 1];
+    q_out.lp[pid * 2] += q[LLP];
+    q_out.lp[pid * 2 + 1] += q[LLP + 1];
     double *Fq = q_out.F + (size_t)pid * 9, *bq = q_out.b + (size_t)pid * 9;
-    Fq[0] += s.d[LF]; Fq[1] += s.d[LF + 1]; Fq[3] += s.d[LF + 2]; Fq[4] += s.d[LF + 3]; Fq[8] += s.d[LF + 4];
-    bq[0] += s.d[LB]; bq[1] += 0.5 * s.d[LB + 1]; bq[3] += 0.5 * s.d[LB + 1]; bq[4] += s.d[LB + 2]; bq[8] += s.d[LB + 3];
-    q_out.E[pid] += s.d[LE];
+    Fq[0] += q[LF]; Fq[1] += q[LF + 1]; Fq[3] += q[LF + 2]; Fq[4] += q[LF + 3]; Fq[8] += q[LF + 4];
+    bq[0] += q[LB]; bq[1] += 0.5 * q[LB + 1]; bq[3] += 0.5 * q[LB + 1]; bq[4] += q[LB + 2]; bq[8] += q[LB + 3];
+    q_out.E[pid] += q[LE];
 }
 
 // A^T with the same (symmetric) block pattern: block (r, c) of A^T is the

@@ -98,13 +98,17 @@ static inline bool vec_ok(const gw_bsr_t *A, const void *u, const void *v) {
 // launch-shape knobs (gw_tune_set): particle CTA, adjoint CTA, warps per CTA
 // of the multigrid row kernels, bound of the dense coarsest level
 inline int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160};
+// block-row kernels: kRowsPerWarp rows per warp (groups of kLPR lanes)
 static inline int tune_rows_grid(int n_rows) {
     const int w = g_tune[GW_TUNE_ROW_WARPS];
-    int b = nblk(n_rows, w);
+    int b = nblk(n_rows, (int64_t)w * kRowsPerWarp);
     return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b);
 }
 static inline int tune_rows_block() { return 32 * g_tune[GW_TUNE_ROW_WARPS]; }
-static inline int red_grid_rows(int n_rows) { int b = nblk(n_rows, kThreads / 32); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
+static inline int red_grid_rows(int n_rows) {
+    int b = nblk(n_rows, (kThreads / 32) * kRowsPerWarp);
+    return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b);
+}
 static inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
 
 static inline LaunchConst make_lc(const gw_grid_t *g, const gw_material_t *m, const gw_step_t *st) {

@@ -128,15 +128,26 @@ __device__ __forceinline__ void load_vec(const double *__restrict__ p, double ou
     }
 }
 
-// One warp per block row; lanes stride over the row's blocks.
+// Block rows are processed by groups of kLPR lanes, kRowsPerWarp rows per
+// warp in flight: the lanes of a group take consecutive blocks of their row
+// (kLPR x 16 bytes per step for 2x2 FP32 blocks: one 128-byte line) and a
+// warp keeps four independent row_ptr -> cols -> x load chains going.  Every
+// lane of a warp runs the same number of row sweeps (rows at or past n_rows
+// are idle groups), so the group shuffles can use the full mask.
+constexpr int kLPR = 8;
+constexpr int kRowsPerWarp = 32 / kLPR;
+
+// acc = (A x)_r summed over the group (valid in the group's first lane); an
+// idle group (r >= n_rows) returns zeros.
 template <int NF, typename VT>
 __device__ __forceinline__ void row_mv(const PtrsA &A, int r, const double *__restrict__ x, double acc[NF]) {
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & (kLPR - 1);
 #pragma unroll
     for (int f = 0; f < NF; ++f) acc[f] = 0.0;
-    const int s = A.row_ptr[r], e = A.row_ptr[r + 1];
+    const int s = r < A.n_rows ? A.row_ptr[r] : 0, e = r < A.n_rows ? A.row_ptr[r + 1] : 0;
     const VT *vals = (const VT *)A.vals;
-    for (int j = s + lane; j < e; j += 32) {
+#pragma unroll 2
+    for (int j = s + lane; j < e; j += kLPR) {
         const int col = A.cols[j];
         if (!in_range(col, A.n_rows, GS_ROW_MV)) continue;
         double xv[NF], bv[NF * NF];
@@ -150,16 +161,17 @@ __device__ __forceinline__ void row_mv(const PtrsA &A, int r, const double *__re
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) acc[f] += __shfl_down_sync(0xffffffffu, acc[f], o);
+        for (int o = kLPR / 2; o > 0; o >>= 1) acc[f] += __shfl_down_sync(0xffffffffu, acc[f], o, kLPR);
 }
 
 template <int NF, typename VT>
 __global__ void k_spmv(PtrsA A, const double *__restrict__ x, double *__restrict__ y) {
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, x, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) y[(size_t)r * NF + f] = acc[f];
     }
@@ -168,14 +180,16 @@ __global__ void k_spmv(PtrsA A, const double *__restrict__ x, double *__restrict
 // y = A^T x (atomic scatter; used by the adjoint)
 template <int NF, typename VT>
 __global__ void k_spmv_t(PtrsA A, const double *__restrict__ x, double *__restrict__ y) {
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    const int lane = threadIdx.x & (kLPR - 1);
     const VT *vals = (const VT *)A.vals;
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
+        if (r >= A.n_rows) continue;  // no shuffles below
         double xr[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) xr[f] = x[(size_t)r * NF + f];
-        for (int j = A.row_ptr[r] + lane; j < A.row_ptr[r + 1]; j += 32) {
+        for (int j = A.row_ptr[r] + lane; j < A.row_ptr[r + 1]; j += kLPR) {
             const int col = A.cols[j];
             if (!in_range(col, A.n_rows, GS_ROW_MV)) continue;
             const VT *blk = vals + (size_t)j * NF * NF;
@@ -275,13 +289,13 @@ struct BicgVecs {
 // r = b - A x ; rh = r ; p = v = 0 ; dots (r,r), (b,b)
 template <int NF, typename VT>
 __global__ void k_bicg_init(PtrsA A, BicgVecs V, double rtol) {
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d[2] = {0.0, 0.0};
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, V.x, acc);
-        if (lane == 0) {
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0) {
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const size_t i = (size_t)r * NF + f;
@@ -326,12 +340,13 @@ __global__ void k_bicg_p(int n_rows, BicgVecs V) {
 template <int NF, typename VT>
 __global__ void k_bicg_v(PtrsA A, BicgVecs V) {
     if (V.sc->done) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d[1] = {0.0};
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, V.y, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const size_t i = (size_t)r * NF + f;
@@ -369,12 +384,13 @@ __global__ void k_bicg_s(int n_rows, BicgVecs V) {
 template <int NF, typename VT>
 __global__ void k_bicg_t(PtrsA A, BicgVecs V) {
     if (V.sc->done) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d[3] = {0.0, 0.0, 0.0};
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, V.z, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const size_t i = (size_t)r * NF + f;
@@ -426,12 +442,13 @@ __global__ void k_bicg_xr(int n_rows, BicgVecs V) {
 // init: r = b - A x ; z = Minv r ; p = z ; rz = (r,z)
 template <int NF, typename VT>
 __global__ void k_cg_init(PtrsA A, BicgVecs V, double rtol) {
-    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d[3] = {0.0, 0.0, 0.0};
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, V.x, acc);
-        if ((threadIdx.x & 31) == 0) {
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0) {
             double rv[NF], zv[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) rv[f] = V.b[(size_t)r * NF + f] - acc[f];
@@ -469,12 +486,13 @@ __global__ void k_cg_p(int n_rows, BicgVecs V) {
 template <int NF, typename VT>
 __global__ void k_cg_q(PtrsA A, BicgVecs V) {
     if (V.sc->done) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d[1] = {0.0};
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, V.p, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const size_t i = (size_t)r * NF + f;
@@ -583,12 +601,13 @@ struct GmresVecs {
 template <int NF, typename VT>
 __global__ void k_gm_residual(PtrsA A, GmresVecs G, int first, double rtol) {
     if (G.sc->done) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     double d[2] = {0.0, 0.0};
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, G.x, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 const size_t i = (size_t)r * NF + f;
@@ -639,11 +658,12 @@ __global__ void k_gm_next(int n_rows, GmresVecs G, int start) {
 template <int NF, typename VT>
 __global__ void k_gm_spmv(PtrsA A, GmresVecs G) {
     if (G.sc->cycle_done) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, G.z, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) G.w[(size_t)r * NF + f] = acc[f];
     }

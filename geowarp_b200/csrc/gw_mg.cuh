@@ -351,11 +351,12 @@ __global__ void k_mg_jacobi(PtrsA A, const double *__restrict__ Minv, const doub
         }
         return;
     }
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, x_in, acc);
-        if ((threadIdx.x & 31) == 0) {
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0) {
             double t[NF], z[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) t[f] = b[(size_t)r * NF + f] - acc[f];
@@ -376,15 +377,16 @@ template <int NF, typename VT>
 __global__ void k_mg_presmooth2(PtrsA A, const double *__restrict__ Minv, const double *__restrict__ b,
                                 double *__restrict__ x_out, double omega, const int *__restrict__ skip) {
     if (skip && *skip) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    const int lane = threadIdx.x & (kLPR - 1);
     const VT *vals = (const VT *)A.vals;
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
 #pragma unroll
         for (int f = 0; f < NF; ++f) acc[f] = 0.0;
-        const int s0 = A.row_ptr[r], e0 = A.row_ptr[r + 1];
-        for (int j = s0 + lane; j < e0; j += 32) {
+        const int s0 = r < A.n_rows ? A.row_ptr[r] : 0, e0 = r < A.n_rows ? A.row_ptr[r + 1] : 0;
+        for (int j = s0 + lane; j < e0; j += kLPR) {
             const int col = A.cols[j];
             if (!in_range(col, A.n_rows, GS_PRESMOOTH)) continue;
             double t[NF], z[NF], bv[NF * NF];
@@ -399,8 +401,8 @@ __global__ void k_mg_presmooth2(PtrsA A, const double *__restrict__ Minv, const 
 #pragma unroll
         for (int f = 0; f < NF; ++f)
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) acc[f] += __shfl_down_sync(0xffffffffu, acc[f], o);
-        if (lane == 0) {
+            for (int o = kLPR / 2; o > 0; o >>= 1) acc[f] += __shfl_down_sync(0xffffffffu, acc[f], o, kLPR);
+        if (r < A.n_rows && lane == 0) {
             double t[NF], z[NF], x1[NF];
 #pragma unroll
             for (int f = 0; f < NF; ++f) t[f] = b[(size_t)r * NF + f];
@@ -421,11 +423,12 @@ template <int NF, typename VT>
 __global__ void k_mg_residual(PtrsA A, const double *__restrict__ b, const double *__restrict__ x,
                               double *__restrict__ r_out, const int *__restrict__ skip) {
     if (skip && *skip) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, x, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) r_out[(size_t)r * NF + f] = b[(size_t)r * NF + f] - acc[f];
     }
@@ -608,7 +611,7 @@ __global__ void k_mg_dense_invert(const double *__restrict__ M, double *__restri
 __global__ void k_mg_dense_apply(const double *__restrict__ Inv, const double *__restrict__ b, double *__restrict__ x,
                                  int n, const int *__restrict__ skip) {
     if (skip && *skip) return;
-    const int nw = gridDim.x * (blockDim.x >> 5);
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
     const int lane = threadIdx.x & 31;
     for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += nw) {
         double s = 0.0;
@@ -639,11 +642,12 @@ __global__ void k_gm_spmv_keep(PtrsA A, GmresVecs G, double *__restrict__ Z) {
     if (G.sc->cycle_done) return;
     if (!in_range(G.sc->k, G.sc->restart, GS_KRYLOV_K)) return;  // Z holds restart vectors
     double *zk = Z + (size_t)G.sc->k * G.n;
-    const int nw = gridDim.x * (blockDim.x >> 5);
-    for (int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < A.n_rows; r += nw) {
+    const int nw = gridDim.x * (blockDim.x >> 5) * kRowsPerWarp;
+    for (int rb = (blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * kRowsPerWarp; rb < A.n_rows; rb += nw) {
+        const int r = rb + (threadIdx.x & 31) / kLPR;
         double acc[NF];
         row_mv<NF, VT>(A, r, G.z, acc);
-        if ((threadIdx.x & 31) == 0)
+        if (r < A.n_rows && (threadIdx.x & (kLPR - 1)) == 0)
 #pragma unroll
             for (int f = 0; f < NF; ++f) {
                 G.w[(size_t)r * NF + f] = acc[f];
