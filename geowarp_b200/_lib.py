@@ -16,7 +16,7 @@ MODEL_HENCKY, MODEL_J2, MODEL_NEOHOOKEAN, MODEL_LINEAR, MODEL_DP, MODEL_NORSAND 
 PREC_F64, PREC_F32 = 0, 1
 PRECOND_DIAG, PRECOND_BLOCK = 0, 1
 KRYLOV_BICGSTAB, KRYLOV_CG, KRYLOV_GMRES = 0, 1, 2
-TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_COUNT = 0, 1, 2, 3, 4
+TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_MG_ONE_SWEEP, TUNE_COUNT = 0, 1, 2, 3, 4, 5
 
 
 class GeoWarpError(RuntimeError):
@@ -106,6 +106,9 @@ SIGNATURES = {
     "gw_set_nodal_pressure": (C.c_int, [C.POINTER(Grid), P, I32, P, P, P, P, P, P]),
     "gw_assemble": (C.c_int, [C.POINTER(Grid), C.POINTER(Material), C.POINTER(Step), C.POINTER(Particles), P, P, P, P,
                               C.POINTER(Bsr), I32, P, P, P]),
+    "gw_assemble_workspace_bytes": (I64, [C.POINTER(Grid), I32, I32]),
+    "gw_assemble_sorted": (C.c_int, [C.POINTER(Grid), C.POINTER(Material), C.POINTER(Step), C.POINTER(Particles), P,
+                                     P, P, P, P, C.POINTER(Bsr), I32, P, P, P, I64, P]),
     "gw_krylov_workspace_bytes": (I64, [I32, I32, I32]),
     "gw_bsr_krylov_solve": (C.c_int, [C.POINTER(Bsr), I32, I32, I32, P, P, C.c_double, I32, P, PI32, PD, P]),
     "gw_krylov_static_max_unknowns": (I64, []),

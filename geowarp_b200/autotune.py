@@ -21,6 +21,7 @@ from . import _lib as L
 KNOBS = {
     "row_warps": (L.TUNE_ROW_WARPS, (2, 4, 8, 16)),
     "mg_coarse": (L.TUNE_MG_COARSE, (40, 80, 160)),
+    "mg_one_sweep": (L.TUNE_MG_ONE_SWEEP, (1, 2, 3, 20)),
     "particle_block": (L.TUNE_PARTICLE_BLOCK, (64, 128, 256)),
     "adjoint_block": (L.TUNE_ADJOINT_BLOCK, (64, 128, 256)),
 }

@@ -304,6 +304,9 @@ extern "C" int gw_tune_set(int32_t knob, int32_t value) {
         case GW_TUNE_MG_COARSE:
             if (value < kMgCoarseMin || value > kMgCoarseMax) return GW_EINVAL;
             break;
+        case GW_TUNE_MG_ONE_SWEEP:
+            if (value < 1 || value > kMgMaxLevels) return GW_EINVAL;
+            break;
         default:
             return GW_EINVAL;
     }

@@ -211,9 +211,10 @@ extern "C" int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t preco
 // ==================================================================== multigrid-preconditioned flexible GMRES
 namespace {
 constexpr double kMgOmega = 0.7;  // damping of the block-Jacobi smoother
-// smoothing sweeps before / after the coarse correction on every level (one
-// sweep on the coarse levels saves launches but costs FP64 Krylov iterations)
-inline int mg_sweeps(int) { return 2; }
+// smoothing sweeps before / after the coarse correction: two, or one from
+// level GW_TUNE_MG_ONE_SWEEP down (fewer launches on the latency-bound coarse
+// levels against more Krylov iterations; the autotuner weighs the two)
+inline int mg_sweeps(int l) { return l >= g_tune[GW_TUNE_MG_ONE_SWEEP] ? 1 : 2; }
 
 // Bump allocator over the caller's workspace; with p == nullptr it only counts,
 // so sizing and carving run the same code.
@@ -555,7 +556,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
 // instantiated graph serves all Newton iterations of a load step.  The graphs
 // are held in a small cache (least recently used entry replaced).
 struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps;
+    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep;
     int n_grid[3];
     int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
     gw_bsr_t A;
@@ -606,6 +607,7 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
     GW_CUDA(cudaGetDevice(&k.device));
     k.nf = NF; k.vt_bytes = sizeof(VT); k.restart = restart; k.nl = h.nl; k.dn = h.dn; k.dim = grid.dim;
     k.row_warps = g_tune[GW_TUNE_ROW_WARPS];
+    k.one_sweep = g_tune[GW_TUNE_MG_ONE_SWEEP];
     for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
     for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
     k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;

@@ -160,6 +160,8 @@ class Engine:
         self.norm_dev = torch.zeros(1, **f64)
         self._sort_ws = _Buf(dev)
         self._scan_ws = _Buf(dev)
+        self._asm_ws = _Buf(dev)  # particle records of the cell-coloured assembly
+        self.deterministic_assembly = True
         self._kry_ws = _Buf(dev)
         self._norm_ws = torch.zeros(16384, dtype=torch.uint8, device=dev)
         self._row_ptr = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -346,12 +348,21 @@ class Engine:
         return st
 
     def assemble(self, mat_struct, current_step, total_steps, want_K=True):
+        """Residual and (want_K) element tangent: the deterministic cell-coloured
+        assembly for the 2D kinds, the atomic one for 3D (or when
+        deterministic_assembly is False)."""
         g, pt, s = self.grid_struct(), self.particles_struct(), self.stream
         st = self.step_struct(current_step, total_steps)
         A = self.bsr_struct()
         if not want_K:
             A.vals = None  # residual only: the row map is still required
         self.force.zero_()
+        if self.D == 2 and self.deterministic_assembly:
+            ws = self._asm_ws.get(L.load().gw_assemble_workspace_bytes(C.byref(g), self.N, self.prec))
+            L.call("gw_assemble_sorted", C.byref(g), C.byref(mat_struct), C.byref(st), C.byref(pt), _p(self.perm),
+                   _p(self.keys), _p(self.free_mask), _p(self.u_new), _p(self.u_old), C.byref(A), self.prec,
+                   _p(self._R), _p(self.force), _p(ws), ws.numel(), s)
+            return
         L.call("gw_assemble", C.byref(g), C.byref(mat_struct), C.byref(st), C.byref(pt), _p(self.perm),
                _p(self.free_mask), _p(self.u_new), _p(self.u_old), C.byref(A), self.prec, _p(self._R),
                _p(self.force), s)

@@ -241,6 +241,22 @@ int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_row2node, i
 int gw_assemble(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st, const gw_particles_t *pt,
                 const int32_t *perm, const uint8_t *free_mask, const double *u_new, const double *u_old,
                 const gw_bsr_t *A, int32_t prec, double *R_rows, double *force, void *stream);
+/* The same residual and tangent for the 2D kinds, bitwise reproducible: the
+ * replacement of the same reference kernels without atomic scatter.  A
+ * particle pass (cell-sorted order, perm and the sorted keys of
+ * gw_cell_sort) evaluates each particle's stress resultants and their
+ * derivatives into workspace records; then one warp per occupied cell sums
+ * its particles' contributions in sorted order into R_rows and A->vals, in
+ * nine colour phases of cells three apart (disjoint node sets: plain
+ * read-modify-writes, no atomics).  Arguments as gw_assemble plus keys (sorted
+ * cell keys), workspace (256-byte aligned) of gw_assemble_workspace_bytes;
+ * the 3D kind falls back to gw_assemble (atomic scatter) and needs no
+ * workspace.  The footing force is still accumulated atomically. */
+int64_t gw_assemble_workspace_bytes(const gw_grid_t *grid, int32_t n_particles, int32_t prec);
+int gw_assemble_sorted(const gw_grid_t *grid, const gw_material_t *mat, const gw_step_t *st,
+                       const gw_particles_t *pt, const int32_t *perm, const int32_t *keys, const uint8_t *free_mask,
+                       const double *u_new, const double *u_old, const gw_bsr_t *A, int32_t prec, double *R_rows,
+                       double *force, void *workspace, int64_t workspace_bytes, void *stream);
 
 /* ------------------------------------------------------------ Krylov
  * Replaces wp.optim.linear.bicgstab with the 'diag' preconditioner and the
@@ -406,17 +422,22 @@ const char *gw_profile_name(int32_t cls);
  *   GW_TUNE_ADJOINT_BLOCK   threads per CTA of the adjoint particle kernels,
  *                           32..256, a multiple of 32 (default 128)
  *   GW_TUNE_ROW_WARPS       warps per CTA of the multigrid smoothing and
- *                           residual kernels (one warp per block row), 1..32
+ *                           residual kernels (four block rows per warp), 1..32
  *                           (default 8)
  *   GW_TUNE_MG_COARSE       most unknowns of the dense coarsest multigrid
  *                           level, 8..160 (default 160)
+ *   GW_TUNE_MG_ONE_SWEEP    first multigrid level smoothed by one sweep
+ *                           before and after the coarse correction instead of
+ *                           two, 1..20 (default 20: two sweeps everywhere);
+ *                           recaptures the step graphs like GW_TUNE_ROW_WARPS
  * gw_tune_set returns GW_EINVAL outside these ranges; gw_tune_get returns -1
  * for an unknown knob. */
 #define GW_TUNE_PARTICLE_BLOCK 0
 #define GW_TUNE_ADJOINT_BLOCK 1
 #define GW_TUNE_ROW_WARPS 2
 #define GW_TUNE_MG_COARSE 3
-#define GW_TUNE_COUNT 4
+#define GW_TUNE_MG_ONE_SWEEP 4
+#define GW_TUNE_COUNT 5
 int gw_tune_set(int32_t knob, int32_t value);
 int32_t gw_tune_get(int32_t knob);
 

@@ -6,7 +6,8 @@ import pytest
 from geowarp_b200 import _lib as L
 from geowarp_b200 import autotune
 
-DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160}
+DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160,
+            L.TUNE_MG_ONE_SWEEP: 20}
 
 
 @pytest.fixture
@@ -23,19 +24,19 @@ def test_knob_defaults_and_ranges(lib):
     assert lib.gw_tune_get(L.TUNE_COUNT) == -1
     bad = [(L.TUNE_PARTICLE_BLOCK, 288), (L.TUNE_PARTICLE_BLOCK, 48), (L.TUNE_ADJOINT_BLOCK, 0),
            (L.TUNE_ROW_WARPS, 0), (L.TUNE_ROW_WARPS, 33), (L.TUNE_MG_COARSE, 7), (L.TUNE_MG_COARSE, 161),
-           (L.TUNE_COUNT, 1)]
+           (L.TUNE_MG_ONE_SWEEP, 0), (L.TUNE_MG_ONE_SWEEP, 21), (L.TUNE_COUNT, 1)]
     for k, v in bad:
         assert lib.gw_tune_set(k, v) == L.GW_EINVAL, (k, v)
         if k != L.TUNE_COUNT:
             assert lib.gw_tune_get(k) == DEFAULTS[k]  # a rejected value leaves the knob alone
     for k, v in [(L.TUNE_PARTICLE_BLOCK, 64), (L.TUNE_ADJOINT_BLOCK, 256), (L.TUNE_ROW_WARPS, 2),
-                 (L.TUNE_MG_COARSE, 40)]:
+                 (L.TUNE_MG_COARSE, 40), (L.TUNE_MG_ONE_SWEEP, 2)]:
         assert lib.gw_tune_set(k, v) == L.GW_OK
         assert lib.gw_tune_get(k) == v
 
 
 def test_coordinate_search_finds_the_separable_optimum(lib):
-    target = {"row_warps": 4, "mg_coarse": 80, "particle_block": 128, "adjoint_block": 64}
+    target = {"row_warps": 4, "mg_coarse": 80, "mg_one_sweep": 2, "particle_block": 128, "adjoint_block": 64}
 
     def cost():
         cfg = autotune.current()
