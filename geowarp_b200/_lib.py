@@ -51,7 +51,7 @@ class Step(C.Structure):
                 ("has_footing", C.c_int32), ("footing_stable", C.c_int32),
                 ("footing_min", C.c_double * 2), ("footing_max", C.c_double * 2),
                 ("footing_initial_height", C.c_double), ("footing_incr_disp", C.c_double),
-                ("penalty_factor", C.c_double), ("gravity_full", C.c_int32), ("pad1", C.c_int32)]
+                ("penalty_factor", C.c_double), ("gravity_full", C.c_int32), ("mobility_law", C.c_int32)]
 
 
 class Particles(C.Structure):
@@ -103,6 +103,7 @@ SIGNATURES = {
     "gw_pattern_count": (C.c_int, [C.POINTER(Grid), P, P, P, I32, P, P, PI32, P, P]),
     "gw_pattern_fill": (C.c_int, [C.POINTER(Grid), C.POINTER(Bsr), P, P]),
     "gw_mass_assemble": (C.c_int, [C.POINTER(Grid), C.POINTER(Particles), P, C.POINTER(Step), C.POINTER(Bsr), P, P]),
+    "gw_mass_lumped_solve": (C.c_int, [C.POINTER(Bsr), P, P, P]),
     "gw_set_nodal_pressure": (C.c_int, [C.POINTER(Grid), P, I32, P, P, P, P, P, P]),
     "gw_assemble": (C.c_int, [C.POINTER(Grid), C.POINTER(Material), C.POINTER(Step), C.POINTER(Particles), P, P, P, P,
                               C.POINTER(Bsr), I32, P, P, P]),

@@ -220,6 +220,14 @@ extern "C" int gw_mass_assemble(const gw_grid_t *grid, const gw_particles_t *pt,
     return GW_OK;
 }
 
+extern "C" int gw_mass_lumped_solve(const gw_bsr_t *M, const double *rhs, double *x, void *stream) {
+    GW_REQUIRE(M && rhs && x && M->nf == 1);
+    if (M->n_rows == 0) return GW_OK;
+    k_mass_lumped<<<gw_count_launch(nblk(M->n_rows, kThreads)), kThreads, 0, S(stream)>>>(make_ptrs(*M), rhs, x);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
 extern "C" int gw_set_nodal_pressure(const gw_grid_t *grid, const int32_t *mass_row2node, int32_t n_mass_rows,
                                      const double *p_hat, const uint8_t *boundary, const uint8_t *node_active,
                                      double *u_old, double *u_new, void *stream) {

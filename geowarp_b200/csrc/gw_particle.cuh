@@ -57,6 +57,25 @@ struct LaunchConst {
     double E0, nu;
 };
 
+// Mobility of the u-p mass balance at the current Jacobian J: the constant
+// k0, or (law 1) Uzuoka & Borja (2012) Eq. 86,
+//   k(J) = k0 (2 mu + lam) J / (mu (1 + J^-2) + (1 - ln J) lam J^-2),
+// with its derivative dk/dJ for the tangent.
+GW_HD double mobility_of(const gw_step_t &st, double J, double lam, double mu, double *dk_dJ) {
+    if (st.mobility_law != 1) {
+        if (dk_dJ) *dk_dJ = 0.0;
+        return st.mobility;
+    }
+    const double iJ2 = 1.0 / (J * J);
+    const double num = (2.0 * mu + lam) * J;
+    const double den = mu * (1.0 + iJ2) + (1.0 - ::log(J)) * lam * iJ2;
+    if (dk_dJ) {
+        const double dden = -iJ2 / J * (2.0 * mu + lam + 2.0 * lam * (1.0 - ::log(J)));
+        *dk_dJ = st.mobility * ((2.0 * mu + lam) * den - num * dden) / (den * den);
+    }
+    return st.mobility * num / den;
+}
+
 // Particle gather results and derived kinematics.
 template <int KIND>
 struct PState {
@@ -331,7 +350,7 @@ GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const doub
         for (int i = 0; i < D; ++i) {
             FtFg[i] = 0.0;
             for (int k = 0; k < D; ++k) FtFg[i] += ev.Finv[k][i] * gsp[k];
-            ev.Q[L::QM2 + i] = V0 * J * c.st.dt * c.st.mobility * FtFg[i];
+            ev.Q[L::QM2 + i] = V0 * J * c.st.dt * mobility_of(c.st, J, ev.lam, ev.mu, nullptr) * FtFg[i];
         }
         const double cold = s.pbar_old - s.pavg_old;
         ev.Q[L::QM3] = V0 * J * tau_ppp * (s.dpt - cold);
@@ -398,7 +417,9 @@ GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const doub
             if (UP) {
                 ev.Dm[L::QS][t] = V0 * dJ;
                 ev.Dm[L::QM1][t] = V0 * dJ * (::log(J) - ::log(ev.J_old) + 1.0);
-                const double fac = V0 * c.st.dt * c.st.mobility;
+                double dmob = 0.0;
+                const double mob = mobility_of(c.st, J, ev.lam, ev.mu, &dmob);
+                const double fac = V0 * c.st.dt;
                 for (int i = 0; i < D; ++i) {
                     double dF = 0.0;
                     if (D == 2) {
@@ -412,7 +433,7 @@ GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const doub
                     } else {
                         for (int m = 0; m < D; ++m) dF += dFinv[m][i] * s.gp[m];
                     }
-                    ev.Dm[L::QM2 + i][t] = fac * (dJ * FtFg[i] + J * dF);
+                    ev.Dm[L::QM2 + i][t] = fac * (dJ * (mob + J * dmob) * FtFg[i] + J * mob * dF);
                 }
                 ev.Dm[L::QM3][t] = V0 * dJ * tau_ppp * (s.dpt - (s.pbar_old - s.pavg_old));
             }
@@ -424,7 +445,7 @@ GW_HD void particle_eval(const LaunchConst &c, const PState<KIND> &s, const doub
         for (int i = 0; i < D; ++i)
             for (int j = 0; j < D; ++j) ev.Dm[L::QU + i * D + j][L::TP] = -V0 * J * ev.Finv[j][i];
         // grad~p lanes
-        const double fac = V0 * J * c.st.dt * c.st.mobility;
+        const double fac = V0 * J * c.st.dt * mobility_of(c.st, J, ev.lam, ev.mu, nullptr);
         for (int i = 0; i < D; ++i)
             for (int k = 0; k < D; ++k) {
                 double v;
@@ -486,7 +507,8 @@ GW_HD void residual_rows(const LaunchConst &c, const PState<KIND> &s, const PEva
             }
         }
         double dot = 0.0;
-        for (int k = 0; k < D; ++k) dot += wg[k] * (c.st.mobility * gsp[k]);
+        const double mob = mobility_of(c.st, ev.J, ev.lam, ev.mu, nullptr);
+        for (int k = 0; k < D; ++k) dot += wg[k] * (mob * gsp[k]);
         double rm = (W * (::log(ev.J) - ::log(ev.J_old)) + dot * c.st.dt) * Vn;
         const double tau_ppp = 0.5 / ev.mu;
         rm += (tau_ppp * (W - Wa) * (s.pbar - s.pavg - (s.pbar_old - s.pavg_old))) * Vn;

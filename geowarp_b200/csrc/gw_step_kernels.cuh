@@ -451,6 +451,17 @@ __global__ void k_identity_dirichlet(PtrsA A, const uint8_t *__restrict__ free_m
 }
 
 // ================================================================ consistent mass
+// Lumped projection: p_i = b_i / sum_j M_ij (the row sum is the lumped nodal
+// mass sum_p N_i m_p by the partition of unity); rows without mass get 0.
+__global__ void k_mass_lumped(PtrsA M, const double *__restrict__ rhs, double *__restrict__ x) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= M.n_rows) return;
+    const double *vals = (const double *)M.vals;
+    double m = 0.0;
+    for (int j = M.row_ptr[r]; j < M.row_ptr[r + 1]; ++j) m += vals[j];
+    x[r] = (m != 0.0) ? rhs[r] / m : 0.0;
+}
+
 template <int KIND>
 __global__ void k_mass(LaunchConst c, PtrsP p, const int *__restrict__ perm, PtrsA M, double *__restrict__ rhs) {
     typedef KindTraits<KIND> KT;

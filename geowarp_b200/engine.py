@@ -32,6 +32,8 @@ MODEL_IDS = {
 }
 
 PRECISIONS = {"fp64": L.PREC_F64, "mixed": L.PREC_F32}
+# u-p mobility: constant k0, or the J-dependent law of Uzuoka & Borja (2012) Eq. 86
+MOBILITY_LAWS = {"constant": 0, "Uzuoka-Borja": 1}
 PRECONDS = {"diag": L.PRECOND_DIAG, "block": L.PRECOND_BLOCK, "mg": "mg"}
 
 
@@ -282,8 +284,9 @@ class Engine:
             self._R = torch.zeros(int(n * 1.25) + 8, dtype=torch.float64, device=self.device)
             self._delta = torch.zeros_like(self._R)
 
-    def project_pressure(self, cg_rtol=1e-13):
-        """Consistent-mass projection of particle pressure to the nodes (GPU CG)."""
+    def project_pressure(self, cg_rtol=1e-13, lumped=False):
+        """Projection of particle pressure to the nodes: consistent mass (GPU
+        CG), or lumped (nodal pressure = sum N m p / sum N m)."""
         g, pt, s = self.grid_struct(), self.particles_struct(), self.stream
         self.touched.zero_()
         L.call("gw_touched_nodes", C.byref(g), _p(self.cell_span), _p(self.touched), s)
@@ -309,13 +312,17 @@ class Engine:
         st = self.step_struct(0, 1)
         L.call("gw_mass_assemble", C.byref(g), C.byref(pt), _p(self.perm), C.byref(st), C.byref(M), _p(self._m_rhs), s)
         self._m_x.zero_()
-        ws = self._kry_ws.get(L.load().gw_krylov_workspace_bytes(self.m_rows, 1, L.PREC_F64))
-        it, rr = C.c_int32(0), C.c_double(0.0)
-        rc = L.load().gw_bsr_krylov_solve(C.byref(M), L.PREC_F64, L.KRYLOV_CG, L.PRECOND_DIAG, _p(self._m_rhs),
-                                          _p(self._m_x), cg_rtol, 100000, _p(ws), C.byref(it), C.byref(rr), s)
-        if rc not in (L.GW_OK, L.GW_ENOCONV):
-            L.check(rc, "consistent-mass CG")
-        self.mass_cg_iters = it.value
+        if lumped:
+            L.call("gw_mass_lumped_solve", C.byref(M), _p(self._m_rhs), _p(self._m_x), s)
+            self.mass_cg_iters = 0
+        else:
+            ws = self._kry_ws.get(L.load().gw_krylov_workspace_bytes(self.m_rows, 1, L.PREC_F64))
+            it, rr = C.c_int32(0), C.c_double(0.0)
+            rc = L.load().gw_bsr_krylov_solve(C.byref(M), L.PREC_F64, L.KRYLOV_CG, L.PRECOND_DIAG, _p(self._m_rhs),
+                                              _p(self._m_x), cg_rtol, 100000, _p(ws), C.byref(it), C.byref(rr), s)
+            if rc not in (L.GW_OK, L.GW_ENOCONV):
+                L.check(rc, "consistent-mass CG")
+            self.mass_cg_iters = it.value
         L.call("gw_set_nodal_pressure", C.byref(g), _p(self.m_row2node), self.m_rows, _p(self._m_x), _p(self.boundary),
                _p(self.node_active), _p(self.u_old), _p(self.u_new), s)
 
@@ -326,6 +333,7 @@ class Engine:
         st.total_steps = float(total_steps)
         st.gravity_mag = float(sp.get("gravity_mag", 0.0))
         st.gravity_full = 0 if sp.get("gravity_ramp", True) else 1
+        st.mobility_law = MOBILITY_LAWS[sp.get("mobility_law", "constant")]
         for k in range(3):
             st.point_load[k] = float(sp.get("point_load", (0.0, 0.0, 0.0))[k])
             st.traction[k] = float(sp.get("traction", (0.0, 0.0, 0.0))[k])

@@ -62,6 +62,15 @@ class quasi_static_coupled_solver_2d:
 
         self.phi_initial = porous_media_dict["phi_initial"]
         self.mobility_constant = porous_media_dict["mobility_constant"]
+        # extensions from the reference's large-deformation consolidation script
+        # (problems/consolidation/large_consolidation_cpGIMP_everything_in_one_script.py):
+        # the J-dependent mobility of :330-338 ("Uzuoka-Borja") and the lumped
+        # pressure projection of :292-310 ("lumped"); the defaults keep the solver
+        # class's own behaviour (constant mobility, consistent-mass projection)
+        self.mobility_law = porous_media_dict.get("mobility_law", "constant")
+        self.p2g_projection = porous_media_dict.get("p2g_projection", "consistent")
+        if self.p2g_projection not in ("consistent", "lumped"):
+            raise ValueError(f"unknown pressure projection {self.p2g_projection!r}")
 
         self.gravity_mag = load_dict["gravity_mag"]
         self.traction_value_x = load_dict.get("traction_value_x", 0.0)
@@ -111,7 +120,7 @@ class quasi_static_coupled_solver_2d:
             gravity_mag=self.gravity_mag, point_load=(self.point_load_value_x, self.point_load_value_y, 0.0),
             traction=(self.traction_value_x, self.traction_value_y, 0.0), p_vol=self.p_vol, p_rho=self.p_rho,
             PPD=self.PPD, lp0=self.GIMP_lp_initial, dt=self.dt, phi_initial=self.phi_initial,
-            mobility=self.mobility_constant)
+            mobility=self.mobility_constant, mobility_law=self.mobility_law)
 
     # ------------------------------------------------------------------ methods
     def reset(self):
@@ -129,7 +138,7 @@ class quasi_static_coupled_solver_2d:
             launch(self.set_boundary_dofs, (self.n_grid_x + 1, self.n_grid_y + 1),
                    [self.dofStruct.boundary_flag_array, self.n_grid_x, self.n_nodes])
         e.sort_and_activate()
-        e.project_pressure()
+        e.project_pressure(lumped=self.p2g_projection == "lumped")
         e.build_system()
         self.newton_iter(current_step, total_steps)
         e.g2p(current_step, total_steps)

@@ -118,7 +118,11 @@ typedef struct gw_step {
     int32_t gravity_full;   /* 0: gravity ramped by (step+1)/total_steps as in the
                                reference; 1: full gravity in every load step (extension,
                                for soil that starts from a geostatic stress state) */
-    int32_t pad1;
+    int32_t mobility_law;   /* u-p: 0 constant mobility (the solver classes); 1 the
+                               J-dependent mobility of Uzuoka & Borja (2012) Eq. 86,
+                               k(J) = k0 (2 mu + lam) J / (mu (1 + J^-2) + (1 - ln J) lam J^-2)
+                               (problems/consolidation/large_consolidation_cpGIMP_
+                               everything_in_one_script.py:330-338, 740) */
 } gw_step_t;
 
 /* Particle state, user order.  x, lp: [N*dim]; F*, b*, sigma: [N*9] row-major
@@ -217,6 +221,11 @@ int gw_pattern_fill(const gw_grid_t *grid, const gw_bsr_t *A, int32_t *cols, voi
  * by particle supports (mass_node2row) and rhs_b. */
 int gw_mass_assemble(const gw_grid_t *grid, const gw_particles_t *pt, const int32_t *perm, const gw_step_t *st,
                      const gw_bsr_t *M, double *rhs, void *stream);
+/* Lumped alternative to the consistent-mass solve: p_i = b_i / sum_j M_ij,
+ * the P2G_solver_lumped kernel of
+ * problems/consolidation/large_consolidation_cpGIMP_everything_in_one_script.py:292-310
+ * (the row sum of M is its lumped nodal mass sum_p N_i m_p). */
+int gw_mass_lumped_solve(const gw_bsr_t *M, const double *rhs, double *x, void *stream);
 /* Writes the projected nodal pressure into the p field of u_old and u_new for
  * non-Dirichlet nodes (and, in 3D, active nodes): P2G_set_nodal_solution(_3d),
  * mpm/mpm_utils.py:387-414. */

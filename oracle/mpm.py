@@ -189,7 +189,8 @@ class OracleEngine:
     """
 
     def __init__(self, kind, grid, x, p_vol, p_rho, PPD, mat, load, lp0, n_iter=10, tol=1e-8, dt=0.0,
-                 phi_initial=0.0, mobility=0.0, E_field=None, act_thresh=None):
+                 phi_initial=0.0, mobility=0.0, E_field=None, act_thresh=None, mobility_law="constant",
+                 p2g_projection="consistent"):
         self.kind = kind
         self.threads = 1  # host threads for the tangent's complex-step passes (timing runs raise it)
         self.D = 2 if kind in ("solid2d", "coupled2d") else 3
@@ -212,6 +213,8 @@ class OracleEngine:
         self.E = np.broadcast_to(np.asarray(E, dtype=np.float64), (self.N,)).copy()
         self.nu = mat["poisson_ratio"]
         self.act_thresh = act_thresh
+        self.mobility_law = mobility_law
+        self.p2g_projection = p2g_projection
         self.F_new = perturbed_identity(self.N)
         self.F_old = perturbed_identity(self.N)
         self.b_new = perturbed_identity(self.N)
@@ -294,7 +297,13 @@ class OracleEngine:
         diag = M.diagonal()
         zero = diag == 0.0
         M = M + sp.diags(zero.astype(np.float64))  # untouched nodes: p_hat = 0
-        xp = spsolve(M.tocsc(), rhs)
+        if self.p2g_projection == "lumped":
+            # P2G_solver_lumped (large_consolidation_cpGIMP_everything_in_one_script.py:292-310):
+            # p_i = sum N m p / sum N m, the lumped mass being the row sum of M
+            msum = np.asarray(M.sum(axis=1)).ravel() - zero  # untouched rows: the unit diagonal added above
+            xp = np.where(msum != 0.0, rhs / np.where(msum != 0.0, msum, 1.0), 0.0)
+        else:
+            xp = spsolve(M.tocsc(), rhs)
         pdof = np.arange(self.n_nodes) + pf * self.n_nodes
         sel = ~self.boundary[pdof]
         if self.kind == "coupled3d":
@@ -388,7 +397,11 @@ class OracleEngine:
                 if pen is not None:
                     r[:, :, D - 1] += pen
             mob = self.mobility
-            r[:, :, pf] = (W * (np.log(J) - np.log(J_old))[:, None]
+            if self.mobility_law == "Uzuoka-Borja":
+                # large_consolidation_cpGIMP_everything_in_one_script.py:330-338 (Eq. 86 of Uzuoka & Borja)
+                mob = mob * ((2.0 * mu + lam) * J) / (mu * (1.0 + 1.0 / J ** 2) + (1.0 - np.log(J)) * lam / J ** 2)
+                mob = mob[:, None]
+            r[:, :, pf] =(W * (np.log(J) - np.log(J_old))[:, None]
                            + np.einsum("nak,nk->na", Ggrad, mob * gradp) * self.dt) * V_new[:, None]
             r[:, :, pf] += (tauppp[:, None] * (W - Wa) * (pbar - pavg - (pbar_old - pavg_old))[:, None]) * V_new[:, None]
         if want_aux:

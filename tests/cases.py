@@ -165,7 +165,9 @@ def oracle_coupled2d(grid, parts, it, mat, porous, load):
               domain_max=(grid["domain_max_x"], grid["domain_max_y"]))
     return OracleEngine("coupled2d", og, x, parts["p_vol"], parts["p_rho"], parts["PPD"], mat, load,
                         lp0=dx / parts["PPD"] / 2.0 - 1e-6, n_iter=it["n_iter"], tol=it["tol"], dt=it["dt"],
-                        phi_initial=porous["phi_initial"], mobility=porous["mobility_constant"])
+                        phi_initial=porous["phi_initial"], mobility=porous["mobility_constant"],
+                        mobility_law=porous.get("mobility_law", "constant"),
+                        p2g_projection=porous.get("p2g_projection", "consistent"))
 
 
 # ---------------------------------------------------------------- 3D u-p: indentation (small)
