@@ -16,7 +16,8 @@ MODEL_HENCKY, MODEL_J2, MODEL_NEOHOOKEAN, MODEL_LINEAR, MODEL_DP, MODEL_NORSAND 
 PREC_F64, PREC_F32 = 0, 1
 PRECOND_DIAG, PRECOND_BLOCK = 0, 1
 KRYLOV_BICGSTAB, KRYLOV_CG, KRYLOV_GMRES = 0, 1, 2
-TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_MG_ONE_SWEEP, TUNE_COUNT = 0, 1, 2, 3, 4, 5
+(TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_MG_ONE_SWEEP, TUNE_MG_SWEEPS,
+ TUNE_MG_OMEGA, TUNE_COUNT) = range(8)
 
 
 class GeoWarpError(RuntimeError):
@@ -74,7 +75,8 @@ MG_MAX_LEVELS = 20
 class MgPlan(C.Structure):
     _fields_ = [("levels", C.c_int32), ("dense_n", C.c_int32), ("n_rows", C.c_int32 * MG_MAX_LEVELS),
                 ("nnzb", C.c_int32 * MG_MAX_LEVELS), ("nf", C.c_int32), ("fine_n_rows", C.c_int32),
-                ("fine_nnzb", C.c_int32), ("lag", C.c_int32), ("workspace", C.c_void_p)]
+                ("fine_nnzb", C.c_int32), ("lag", C.c_int32), ("workspace", C.c_void_p),
+                ("row_ptr", C.c_void_p), ("cols", C.c_void_p), ("last_iters", C.c_int32), ("pad0", C.c_int32)]
 
 
 class Adjoint(C.Structure):

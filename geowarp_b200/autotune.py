@@ -17,11 +17,14 @@ import statistics
 
 from . import _lib as L
 
-# knob name -> (gw_tune_set id, candidates searched)
+# knob name -> (gw_tune_set id, candidates searched).  The multigrid smoother
+# knobs (GW_TUNE_MG_SWEEPS / _OMEGA / _ONE_SWEEP) are not searched: on the
+# workloads here two sweeps at 0.7 on every level were fastest, and damping of
+# 0.8 and above makes the block-Jacobi smoother diverge (GMRES then runs to
+# its iteration cap).
 KNOBS = {
     "row_warps": (L.TUNE_ROW_WARPS, (2, 4, 8, 16)),
     "mg_coarse": (L.TUNE_MG_COARSE, (40, 80, 160)),
-    "mg_one_sweep": (L.TUNE_MG_ONE_SWEEP, (1, 2, 3, 20)),
     "particle_block": (L.TUNE_PARTICLE_BLOCK, (64, 128, 256)),
     "adjoint_block": (L.TUNE_ADJOINT_BLOCK, (64, 128, 256)),
 }
@@ -67,14 +70,22 @@ def tune(trial, reps=3, knobs=KNOBS, timer=cuda_timer, log=None):
     other knobs at their best so far), trial() runs once untimed and then reps
     times under timer; the candidate with the smallest median stays set.
     Returns (best config, {knob: {candidate: median ms}})."""
+    import time
     best = current(knobs)
     table = {}
+    best_ms = None
     for name, (k, cands) in knobs.items():
         times = {}
         for v in cands:
             L.call("gw_tune_set", k, int(v))
+            t0 = time.perf_counter()
             trial()
-            times[v] = statistics.median(timer(trial) for _ in range(reps))
+            first_ms = 1e3 * (time.perf_counter() - t0)
+            if best_ms is not None and first_ms > 4.0 * best_ms + 50.0:
+                times[v] = first_ms  # far slower already untimed: not repeated
+            else:
+                times[v] = statistics.median(timer(trial) for _ in range(reps))
+                best_ms = times[v] if best_ms is None else min(best_ms, times[v])
             if log:
                 log(f"autotune {name}={v}: {times[v]:.3f} ms")
         pick = min(times, key=times.get)

@@ -315,6 +315,12 @@ extern "C" int gw_tune_set(int32_t knob, int32_t value) {
         case GW_TUNE_MG_ONE_SWEEP:
             if (value < 1 || value > kMgMaxLevels) return GW_EINVAL;
             break;
+        case GW_TUNE_MG_SWEEPS:
+            if (value < 1 || value > 4) return GW_EINVAL;
+            break;
+        case GW_TUNE_MG_OMEGA:
+            if (value < 10 || value > 100) return GW_EINVAL;
+            break;
         default:
             return GW_EINVAL;
     }

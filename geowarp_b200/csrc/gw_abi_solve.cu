@@ -210,11 +210,12 @@ extern "C" int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t preco
 
 // ==================================================================== multigrid-preconditioned flexible GMRES
 namespace {
-constexpr double kMgOmega = 0.7;  // damping of the block-Jacobi smoother
+// damping of the block-Jacobi smoother (GW_TUNE_MG_OMEGA, in percent)
+inline double mg_omega() { return 0.01 * g_tune[GW_TUNE_MG_OMEGA]; }
 // smoothing sweeps before / after the coarse correction: two, or one from
 // level GW_TUNE_MG_ONE_SWEEP down (fewer launches on the latency-bound coarse
 // levels against more Krylov iterations; the autotuner weighs the two)
-inline int mg_sweeps(int l) { return l >= g_tune[GW_TUNE_MG_ONE_SWEEP] ? 1 : 2; }
+inline int mg_sweeps(int l) { return l >= g_tune[GW_TUNE_MG_ONE_SWEEP] ? 1 : g_tune[GW_TUNE_MG_SWEEPS]; }
 
 // Bump allocator over the caller's workspace; with p == nullptr it only counts,
 // so sizing and carving run the same code.
@@ -404,6 +405,8 @@ int mg_pattern(MgHier &h, const gw_bsr_t *A0, gw_mg_plan_t *plan, cudaStream_t s
     plan->nf = NF;
     plan->fine_n_rows = A0->n_rows;
     plan->fine_nnzb = A0->nnzb;
+    plan->row_ptr = A0->row_ptr;
+    plan->cols = A0->cols;
     return GW_OK;
 }
 
@@ -480,8 +483,8 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
     const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
     ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
                  2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
-    if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
-    else k_mg_jacobi<NF, double><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, kMgOmega, zero, skip);
+    if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
+    else k_mg_jacobi<NF, double><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
 }
 
 // One V-cycle on h.lv[0].b; returns the buffer that holds the result (the same
@@ -494,7 +497,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
     for (int l = 0; l < last; ++l) {
         const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
         double *x = v.x, *y = v.x2;
-        if (mg_sweeps(l) == 2) {
+        if (mg_sweeps(l) >= 2) {
             // both zero-start sweeps in one launch, into the buffer the
             // second separate sweep would have written
             PtrsA a = make_ptrs(v.A);
@@ -503,11 +506,15 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
             ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
             if (l == 0)
                 k_mg_presmooth2<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
-                    a, v.Minv, v.b, y, kMgOmega, skip);
+                    a, v.Minv, v.b, y, mg_omega(), skip);
             else
                 k_mg_presmooth2<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
-                    a, v.Minv, v.b, y, kMgOmega, skip);
+                    a, v.Minv, v.b, y, mg_omega(), skip);
             double *t = x; x = y; y = t;
+            for (int it = 2; it < mg_sweeps(l); ++it) {
+                mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
+                t = x; x = y; y = t;
+            }
         } else {
             mg_jacobi<NF, VT>(h, l, v.b, nullptr, x, 1, skip, s);
             for (int it = 1; it < mg_sweeps(l); ++it) {
@@ -556,7 +563,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
 // instantiated graph serves all Newton iterations of a load step.  The graphs
 // are held in a small cache (least recently used entry replaced).
 struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep;
+    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega;
     int n_grid[3];
     int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
     gw_bsr_t A;
@@ -572,7 +579,6 @@ struct MgGraphEntry {
     uint64_t stamp;
 };
 constexpr int kMgGraphCache = 8;
-int g_gm_last_iters = 0;  // iterations of the previous multigrid GMRES solve (first-chunk hint)
 MgGraphEntry g_mg_graphs[kMgGraphCache];
 uint64_t g_mg_graph_clock = 0;
 cudaStream_t g_capture_stream[64] = {};
@@ -608,6 +614,8 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
     k.nf = NF; k.vt_bytes = sizeof(VT); k.restart = restart; k.nl = h.nl; k.dn = h.dn; k.dim = grid.dim;
     k.row_warps = g_tune[GW_TUNE_ROW_WARPS];
     k.one_sweep = g_tune[GW_TUNE_MG_ONE_SWEEP];
+    k.sweeps = g_tune[GW_TUNE_MG_SWEEPS];
+    k.omega = g_tune[GW_TUNE_MG_OMEGA];
     for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
     for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
     k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;
@@ -653,7 +661,7 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
 }
 
 template <int NF, typename VT>
-int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_in, const double *b, double *x,
+int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, const double *b, double *x,
              double rtol, int max_iter, int restart, void *ws, int64_t ws_bytes, int *iters, double *relres,
              cudaStream_t s) {
     const int nr = A->n_rows;
@@ -675,7 +683,8 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
         gw_mg_plan_t local;
         if (plan_in) {
             if (plan_in->workspace != ws || plan_in->nf != NF || plan_in->fine_n_rows != nr ||
-                plan_in->fine_nnzb != A->nnzb || plan_in->levels < 1 || plan_in->levels > h.nl ||
+                plan_in->fine_nnzb != A->nnzb || plan_in->row_ptr != A->row_ptr || plan_in->cols != A->cols ||
+                plan_in->levels < 1 || plan_in->levels > h.nl ||
                 plan_in->dense_n != plan_in->n_rows[plan_in->levels - 1] * NF || plan_in->dense_n > kMgCoarseMax) {
                 snprintf(g_msg, sizeof(g_msg), "multigrid GMRES: the plan was built for another workspace or pattern");
                 return GW_EINVAL;
@@ -719,7 +728,8 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
         // alike), then the iterations left at the observed convergence rate.
         // Steps queued past convergence still launch their (early-exiting)
         // kernels, so the estimate trims them without adding host reads.
-        int chunk = g_gm_last_iters > 0 ? std::min(std::max(g_gm_last_iters, 2), 16) : 4;
+        const int hint = plan_in ? plan_in->last_iters : 0;
+        int chunk = hint > 0 ? std::min(std::max(hint, 2), 16) : 4;
         int kk = 0;
         const double spmv_bytes = (double)A->nnzb * (NF * NF * sizeof(VT) + 4) + 4.0 * (nr + 1) + 24.0 * n;
         cudaGraphExec_t step_graph = nullptr;
@@ -766,7 +776,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
     }
     *iters = hs.iters;
     *relres = (hs.bnorm > 0.0) ? hs.resid / hs.bnorm : 0.0;
-    g_gm_last_iters = hs.iters;
+    if (plan_in) plan_in->last_iters = hs.iters;
     rc = guard_check(s, "multigrid GMRES");
     if (rc) return rc;
     if (hs.status == ST_NAN) return GW_ENAN;
@@ -775,7 +785,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan_
 }
 
 template <typename VT>
-int gmres_mg_nf(const gw_grid_t *grid, const gw_bsr_t *A, const gw_mg_plan_t *plan, const double *b, double *x,
+int gmres_mg_nf(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan, const double *b, double *x,
                 double rtol, int max_iter, int restart, void *ws, int64_t ws_bytes, int *iters, double *relres,
                 cudaStream_t s) {
     switch (A->nf) {
@@ -829,7 +839,7 @@ extern "C" int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *
 }
 
 extern "C" int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec,
-                                     const gw_mg_plan_t *plan_host, const double *b, double *x, double rtol,
+                                     gw_mg_plan_t *plan_host, const double *b, double *x, double rtol,
                                      int32_t max_iter, int32_t restart, void *workspace, int64_t workspace_bytes,
                                      int32_t *iters_host, double *relres_host, void *stream) {
     GW_REQUIRE(grid && A && b && x && workspace && iters_host && relres_host && max_iter > 0);

@@ -173,6 +173,7 @@ class Engine:
         self._delta = torch.zeros(1, **f64)
         self._mg_plan = None
         self._mg_numeric = None  # (role of the last numeric phase, its GMRES iterations)
+        self._gm_hint = 0  # iterations of this engine's last multigrid GMRES solve
         self.mg_lag = True  # Newton solves of a load step share one multigrid numeric phase
         # consistent-mass system (u-p kinds)
         if self.nf > self.D:
@@ -422,6 +423,7 @@ class Engine:
                 # coarse patterns: once per load step (the pattern is fixed within it)
                 plan = L.MgPlan()
                 L.call("gw_mg_plan_build", C.byref(g), C.byref(A), _p(ws), ws.numel(), C.byref(plan), self.stream)
+                plan.last_iters = self._gm_hint  # first Arnoldi chunk: this engine's previous solve
                 self._mg_plan = plan
                 self._mg_numeric = None
             plan.lag = int(bool(self.mg_lag and newton and self._mg_numeric is not None
@@ -429,6 +431,7 @@ class Engine:
             rc = lib.gw_bsr_gmres_mg_solve(C.byref(g), C.byref(A), self.prec, C.byref(plan), _p(b), _p(x), rtol,
                                            self.krylov_max_iter, self.restart, _p(ws), ws.numel(), C.byref(it),
                                            C.byref(rr), self.stream)
+            self._gm_hint = plan.last_iters
             if not newton:
                 self._mg_numeric = ("other", it.value)
             elif not plan.lag:

@@ -287,8 +287,10 @@ int gw_bsr_krylov_solve(const gw_bsr_t *A, int32_t prec, int32_t method, int32_t
  * n_rows * nf <= gw_krylov_static_max_unknowns() (131072); larger systems
  * return GW_EINVAL with a message naming the limit.  The first call on a
  * device looks up the array's device address with that device current (the
- * stream must belong to the current device); make that first call before any
- * stream capture.  All calls on a device share the one array: every call
+ * stream must belong to the current device) and keeps it for the life of the
+ * process; make that first call before any stream capture, and do not reset
+ * the device (cudaDeviceReset) after it, since the kept address would then be
+ * stale.  All calls on a device share the one array: every call
  * clears the part that must start at zero, but calls that overlap on the GPU
  * (other streams, other host threads) race on it and must be serialised by
  * the caller. */
@@ -332,7 +334,12 @@ int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const d
  * pattern and role, e.g. the previous Newton iterate's Jacobian), while
  * GMRES applies A itself, so the solution is A's; only the preconditioner
  * lags.  The caller must have run one solve with lag = 0 on this plan and
- * workspace first. */
+ * workspace first.  A plan is accepted only for the pattern it was built from:
+ * the same workspace, row count, block count and row_ptr / cols arrays
+ * (GW_EINVAL otherwise).  The solve writes its iteration count to
+ * plan_host->last_iters: the next solve with the plan queues that many
+ * Arnoldi steps before its first host check (a caller that rebuilds the plan
+ * may carry the value over). */
 #define GW_MG_MAX_LEVELS 20
 typedef struct gw_mg_plan {
     int32_t levels;                     /* levels holding a matrix; the last one is solved densely */
@@ -342,11 +349,14 @@ typedef struct gw_mg_plan {
     int32_t nf, fine_n_rows, fine_nnzb;
     int32_t lag;                        /* 1: reuse the previous solve's numeric phase (see above)  */
     const void *workspace;              /* the coarse patterns live in this workspace              */
+    const void *row_ptr, *cols;         /* pattern arrays of the matrix the plan was built from    */
+    int32_t last_iters;                 /* iterations of the last solve with this plan (0: none)    */
+    int32_t pad0;
 } gw_mg_plan_t;
 int64_t gw_gmres_mg_workspace_bytes(const gw_grid_t *grid, int32_t n_rows, int32_t nf, int32_t restart);
 int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *workspace, int64_t workspace_bytes,
                      gw_mg_plan_t *plan_host, void *stream);
-int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, const gw_mg_plan_t *plan_host,
+int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, gw_mg_plan_t *plan_host,
                           const double *b, double *x, double rtol, int32_t max_iter, int32_t restart, void *workspace,
                           int64_t workspace_bytes, int32_t *iters_host, double *relres_host, void *stream);
 /* y = A x (x, y FP64 of length n_rows*nf; A values in prec). */
@@ -437,8 +447,14 @@ const char *gw_profile_name(int32_t cls);
  *                           level, 8..160 (default 160)
  *   GW_TUNE_MG_ONE_SWEEP    first multigrid level smoothed by one sweep
  *                           before and after the coarse correction instead of
- *                           two, 1..20 (default 20: two sweeps everywhere);
+ *                           GW_TUNE_MG_SWEEPS, 1..20 (default 20: none);
  *                           recaptures the step graphs like GW_TUNE_ROW_WARPS
+ *   GW_TUNE_MG_SWEEPS       block-Jacobi sweeps before and after the coarse
+ *                           correction on the other levels, 1..4 (default 2)
+ *   GW_TUNE_MG_OMEGA        damping of those sweeps in percent, 10..100
+ *                           (default 70)
+ * The last two change the preconditioner (Krylov iteration counts), not the
+ * solution GMRES converges to; they also recapture the step graphs.
  * gw_tune_set returns GW_EINVAL outside these ranges; gw_tune_get returns -1
  * for an unknown knob. */
 #define GW_TUNE_PARTICLE_BLOCK 0
@@ -446,7 +462,9 @@ const char *gw_profile_name(int32_t cls);
 #define GW_TUNE_ROW_WARPS 2
 #define GW_TUNE_MG_COARSE 3
 #define GW_TUNE_MG_ONE_SWEEP 4
-#define GW_TUNE_COUNT 5
+#define GW_TUNE_MG_SWEEPS 5
+#define GW_TUNE_MG_OMEGA 6
+#define GW_TUNE_COUNT 7
 int gw_tune_set(int32_t knob, int32_t value);
 int32_t gw_tune_get(int32_t knob);
 

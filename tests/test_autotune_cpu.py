@@ -7,7 +7,7 @@ from geowarp_b200 import _lib as L
 from geowarp_b200 import autotune
 
 DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160,
-            L.TUNE_MG_ONE_SWEEP: 20}
+            L.TUNE_MG_ONE_SWEEP: 20, L.TUNE_MG_SWEEPS: 2, L.TUNE_MG_OMEGA: 70}
 
 
 @pytest.fixture
@@ -24,7 +24,8 @@ def test_knob_defaults_and_ranges(lib):
     assert lib.gw_tune_get(L.TUNE_COUNT) == -1
     bad = [(L.TUNE_PARTICLE_BLOCK, 288), (L.TUNE_PARTICLE_BLOCK, 48), (L.TUNE_ADJOINT_BLOCK, 0),
            (L.TUNE_ROW_WARPS, 0), (L.TUNE_ROW_WARPS, 33), (L.TUNE_MG_COARSE, 7), (L.TUNE_MG_COARSE, 161),
-           (L.TUNE_MG_ONE_SWEEP, 0), (L.TUNE_MG_ONE_SWEEP, 21), (L.TUNE_COUNT, 1)]
+           (L.TUNE_MG_ONE_SWEEP, 0), (L.TUNE_MG_ONE_SWEEP, 21), (L.TUNE_MG_SWEEPS, 5), (L.TUNE_MG_OMEGA, 101),
+           (L.TUNE_COUNT, 1)]
     for k, v in bad:
         assert lib.gw_tune_set(k, v) == L.GW_EINVAL, (k, v)
         if k != L.TUNE_COUNT:
@@ -36,7 +37,7 @@ def test_knob_defaults_and_ranges(lib):
 
 
 def test_coordinate_search_finds_the_separable_optimum(lib):
-    target = {"row_warps": 4, "mg_coarse": 80, "mg_one_sweep": 2, "particle_block": 128, "adjoint_block": 64}
+    target = {"row_warps": 4, "mg_coarse": 80, "particle_block": 128, "adjoint_block": 64}
 
     def cost():
         cfg = autotune.current()

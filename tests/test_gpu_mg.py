@@ -138,6 +138,15 @@ def test_mg_plan_reuse_and_rejection(cuda):
         assert rc == 0
         xs.append(x.cpu().numpy())
     assert np.array_equal(xs[0], xs[1])
+    assert plan.last_iters > 0  # the solve leaves its iteration count in the plan
+    # a matrix with other pattern arrays (a copy of the column array) is refused
+    cols2 = e._cols.clone()
+    A2 = e.bsr_struct()
+    A2.cols = _p(cols2)
+    x = torch.zeros(n, dtype=torch.float64, device=e.device)
+    rc = lib.gw_bsr_gmres_mg_solve(C.byref(g), C.byref(A2), e.prec, C.byref(plan), _p(e._R), _p(x), 1e-10, 500,
+                                   30, _p(ws), nbytes, C.byref(it), C.byref(rr), e.stream)
+    assert rc == L.GW_EINVAL
     ws2 = torch.zeros(nbytes, dtype=torch.uint8, device=e.device)
     x = torch.zeros(n, dtype=torch.float64, device=e.device)
     it, rr = C.c_int32(0), C.c_double(0.0)
