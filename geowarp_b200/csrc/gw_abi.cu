@@ -20,7 +20,9 @@ extern "C" int gw_guard_read(int32_t *site, int64_t *value, void *stream) {
     GW_CUDA(cudaMemcpyFromSymbolAsync(&v, g_guard_value, sizeof(long long), 0, cudaMemcpyDeviceToHost, s));
     GW_CUDA(cudaStreamSynchronize(s));
     const int zero = 0;
+    const long long zero_v = 0;
     GW_CUDA(cudaMemcpyToSymbolAsync(g_guard_site, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+    GW_CUDA(cudaMemcpyToSymbolAsync(g_guard_value, &zero_v, sizeof(long long), 0, cudaMemcpyHostToDevice, s));
     GW_CUDA(cudaStreamSynchronize(s));
     *site = st;
     *value = v;
@@ -42,7 +44,7 @@ extern "C" const char *gw_status_string(int code) {
         case GW_ENOCONV: return "Krylov solver did not reach the tolerance";
         case GW_EBREAKDOWN: return "Krylov breakdown";
         case GW_ENAN: return "non-finite value";
-        case GW_ERANGE: return "particle support outside the background grid";
+        case GW_ERANGE: return g_msg[0] ? g_msg : "index guard failed: a device index was out of range";
         case GW_EMODEL: return "material model not available for this solver kind";
         default: return "unknown status";
     }

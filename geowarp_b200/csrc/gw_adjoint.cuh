@@ -15,9 +15,11 @@
 // They come from forward-mode dual passes through the same formulas as the
 // forward kernels, chunked: each pass carries kAdjChunk dual lanes (a window
 // of the inputs) and contracts every output with its weight as soon as it is
-// formed, so no per-row Jacobian is kept and a pass fits in registers.  The
-// 19 inputs take four passes (the residual adjoint, which needs inputs 0-13
-// only, takes three).
+// formed, so no per-row Jacobian is kept.  The 19 inputs take seven passes
+// (the residual adjoint, which needs inputs 0-13 only, takes five).  The
+// principal-space constitutive update (eigen-solve and return map) runs once
+// per particle, before the passes, as a 5-lane Jacobian with respect to the
+// trial b and E (constitutive_jac); the passes apply it by the chain rule.
 #pragma once
 #include "gw_step_kernels.cuh"
 
@@ -74,13 +76,14 @@ GW_HD void gimp_axis_dual(const AD &xp, const AD &lp, double d, double inv_d, in
 // fA carries the lanes of the principal values (through the return map), the
 // off-diagonal lanes are D_AB (V^T db V)_AB with D_AB = (f_A - f_B)/(l_A - l_B)
 // or its coalescence limit lim_AB.
-GW_HD void spectral_assemble(const double V[3][3], const double lamb[3], const AD fA[3], const double lim[3][3],
-                             const double dbp[][3][3], AD out[3][3]) {
+template <int NL>
+GW_HD void spectral_assemble(const double V[3][3], const double lamb[3], const Dual<NL, double> fA[3],
+                             const double lim[3][3], const double dbp[][3][3], Dual<NL, double> out[3][3]) {
     for (int i = 0; i < 3; ++i)
         for (int j = 0; j < 3; ++j) {
             double v = 0.0;
             for (int A = 0; A < 3; ++A) v += fA[A].v * V[i][A] * V[j][A];
-            out[i][j] = AD(v);
+            out[i][j] = Dual<NL, double>(v);
         }
     double D[3][3];
     for (int A = 0; A < 3; ++A)
@@ -90,7 +93,7 @@ GW_HD void spectral_assemble(const double V[3][3], const double lamb[3], const A
             const double sc = fmax(fabs(lamb[A]), fabs(lamb[B]));
             D[A][B] = (fabs(dl) > 1e-9 * sc) ? (fA[A].v - fA[B].v) / dl : lim[A][B];
         }
-    for (int l = 0; l < kAdjLanes; ++l) {
+    for (int l = 0; l < NL; ++l) {
         double M[3][3];
         for (int A = 0; A < 3; ++A)
             for (int B = 0; B < 3; ++B) M[A][B] = (A == B) ? fA[A].d[l] : D[A][B] * dbp[l][A][B];
@@ -102,6 +105,144 @@ GW_HD void spectral_assemble(const double V[3][3], const double lamb[3], const A
                 out[i][j].d[l] = v;
             }
     }
+}
+
+// Principal return map of the principal-space models (Hencky, J2,
+// Drucker-Prager) with its algorithmic tangent: lanes 0..2 seed the trial
+// principal log strains, lane 3 seeds E (through lam and mu).
+template <int MODEL>
+GW_HD void principal_tangent_E(const LaunchConst &c, int model, double Ev, const double etr_v[3], double tau_v[3],
+                               double dtau[3][4], double e_v[3], double de[3][4]) {
+    typedef Dual<4, double> T;
+    const double nu = c.nu;
+    T E(Ev);
+    E.d[3] = 1.0;
+    const T lam = E * (nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
+    const T mu = E * (1.0 / (2.0 * (1.0 + nu)));
+    T etr[3], e[3], tau[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        etr[i] = T(etr_v[i]);
+        etr[i].d[i] = 1.0;
+    }
+    if (model == GW_MODEL_J2) rm_j2<T, double, T>(etr, lam, mu, c.mc.kappa, e);
+    else if (model == GW_MODEL_DP) rm_dp<T, double, T>(etr, lam, mu, c.mc, e);
+    else
+        for (int i = 0; i < 3; ++i) e[i] = etr[i];
+    tau_hencky(e, lam, mu, tau);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        tau_v[i] = tau[i].v;
+        e_v[i] = e[i].v;
+#pragma unroll
+        for (int l = 0; l < 4; ++l) {
+            dtau[i][l] = tau[i].d[l];
+            de[i][l] = e[i].d[l];
+        }
+    }
+}
+
+// Jacobian of the principal-space constitutive update of one particle,
+// evaluated once per particle: tau and b_new (plane-strain components 00,
+// 01 = 10, 11, 22) with respect to the trial b's components (00, 01 = 10,
+// 11, 22; a symmetric perturbation of the 01 / 10 pair) and E.  The trial b
+// is eigen-decomposed once, each direction is rotated into its frame, the
+// principal derivatives come from the return map's algorithmic tangent, and
+// the isotropic tensor functions are assembled back with their coalescence
+// limits.  Every chunked pass then takes tau's and b_new's lanes from this
+// record by the chain rule, so the eigen-solve and the return map run once
+// per particle instead of once per pass.
+constexpr int kCJ = 5;
+struct ConstJac {
+    double tv[4], Jt[4][kCJ];  // tau
+    double bv[4], Jb[4][kCJ];  // b_new (G2P adjoint only)
+};
+
+template <int MODEL>
+GW_HD void constitutive_jac(const LaunchConst &c, int model, const double B[3][3], double Ev, bool want_b,
+                            ConstJac &cj) {
+    typedef Dual<kCJ, double> CD;
+    double lamb[3], V[3][3], Bc[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) Bc[i][j] = B[i][j];
+    eig_sym3(Bc, lamb, V);
+    // directions 0..3: unit symmetric perturbations of b_trial 00, 01/10, 11, 22, rotated: V^T dB V
+    double dbp[kCJ][3][3];
+    const int pi[4] = {0, 0, 1, 2}, pj[4] = {0, 1, 1, 2};
+    for (int k = 0; k < kCJ; ++k)
+        for (int A = 0; A < 3; ++A)
+            for (int Bq = 0; Bq < 3; ++Bq) {
+                double v = 0.0;
+                if (k < 4) {
+                    const int i = pi[k], j = pj[k];
+                    v = V[i][A] * V[j][Bq];
+                    if (i != j) v += V[j][A] * V[i][Bq];
+                }
+                dbp[k][A][Bq] = v;
+            }
+    double etr_v[3], tv[3], dtau[3][4], ev[3], de[3][4];
+    bool ok[3];
+    for (int A = 0; A < 3; ++A) {
+        ok[A] = lamb[A] > 1e-8;
+        etr_v[A] = 0.5 * ::log(ok[A] ? lamb[A] : 1e-8);
+    }
+    principal_tangent_E<MODEL>(c, model, Ev, etr_v, tv, dtau, ev, de);
+    CD fA[3], fB[3];
+    double limT[3][3], limB[3][3];
+    for (int A = 0; A < 3; ++A) {
+        const double fb = ::exp(2.0 * ev[A]);
+        fA[A] = CD(tv[A]);
+        fB[A] = CD(fb);
+        for (int k = 0; k < kCJ; ++k) {
+            double dt = (k == 4) ? dtau[A][3] : 0.0, dl = (k == 4) ? de[A][3] : 0.0;
+            for (int Bq = 0; Bq < 3; ++Bq) {
+                const double detr = ok[Bq] ? dbp[k][Bq][Bq] / (2.0 * lamb[Bq]) : 0.0;
+                dt += dtau[A][Bq] * detr;
+                dl += de[A][Bq] * detr;
+            }
+            fA[A].d[k] = dt;
+            fB[A].d[k] = 2.0 * fb * dl;
+        }
+        for (int Bq = 0; Bq < 3; ++Bq) {
+            limT[A][Bq] = (dtau[A][A] - dtau[A][Bq]) / (2.0 * lamb[A]);
+            limB[A][Bq] = 2.0 * fb * (de[A][A] - de[A][Bq]) / (2.0 * lamb[A]);
+        }
+    }
+    CD out[3][3];
+    spectral_assemble<kCJ>(V, lamb, fA, limT, dbp, out);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        cj.tv[k] = out[pi[k]][pj[k]].v;
+        for (int l = 0; l < kCJ; ++l) cj.Jt[k][l] = out[pi[k]][pj[k]].d[l];
+    }
+    if (!want_b) return;
+    spectral_assemble<kCJ>(V, lamb, fB, limB, dbp, out);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        cj.bv[k] = out[pi[k]][pj[k]].v;
+        for (int l = 0; l < kCJ; ++l) cj.Jb[k][l] = out[pi[k]][pj[k]].d[l];
+    }
+}
+
+// out (tau or b_new) with this pass's lanes: value from the Jacobian record,
+// lanes = J (d b_trial components, d E).
+GW_HD void apply_cjac(const double v[4], const double J[4][kCJ], const AD btr[3][3], const AD &E, AD out[3][3]) {
+    AD q[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        q[k] = AD(v[k]);
+#pragma unroll
+        for (int l = 0; l < kAdjLanes; ++l)
+            q[k].d[l] = J[k][0] * btr[0][0].d[l] + J[k][1] * btr[0][1].d[l] + J[k][2] * btr[1][1].d[l] +
+                        J[k][3] * btr[2][2].d[l] + J[k][4] * E.d[l];
+    }
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) out[i][j] = AD(0.0);
+    out[0][0] = q[0];
+    out[0][1] = q[1];
+    out[1][0] = q[1];
+    out[1][1] = q[2];
+    out[2][2] = q[3];
 }
 
 // Weights of the contracted outputs: lambda per slot and field for the
@@ -127,7 +268,7 @@ struct SolidDual {
 template <int MODEL>
 GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lpv, const double *Fo_v,
                         const double *bo_v, double Ev, const double fext[2], const double du[9][2], int off,
-                        const DualWeights &wt, SolidDual &o) {
+                        const DualWeights &wt, ConstJac &cj, SolidDual &o) {
     const gw_grid_t &g = c.g;
     const bool want_g2p = wt.x != nullptr;
     o.s = AD(0.0);
@@ -196,47 +337,10 @@ GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lp
     AD tau[3][3];
     const int model = MODEL >= 0 ? MODEL : c.mc.model;
     if (model == GW_MODEL_HENCKY || model == GW_MODEL_J2 || model == GW_MODEL_DP) {
-        double B[3][3], lamb[3], V[3][3];
-        for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) B[i][j] = btr[i][j].v;
-        eig_sym3(B, lamb, V);
-        double dbp[kAdjLanes][3][3];
-        for (int l = 0; l < kAdjLanes; ++l) {
-            double T1[3][3];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j)
-                    T1[i][j] = btr[i][0].d[l] * V[0][j] + btr[i][1].d[l] * V[1][j] + btr[i][2].d[l] * V[2][j];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) dbp[l][i][j] = V[0][i] * T1[0][j] + V[1][i] * T1[1][j] + V[2][i] * T1[2][j];
-        }
-        AD etr[3], e[3], tA[3];
-        double etr_v[3];
-        for (int A = 0; A < 3; ++A) {
-            const bool ok = lamb[A] > 1e-8;
-            etr_v[A] = 0.5 * ::log(ok ? lamb[A] : 1e-8);
-            etr[A] = AD(etr_v[A]);
-            for (int l = 0; l < kAdjLanes; ++l) etr[A].d[l] = ok ? dbp[l][A][A] / (2.0 * lamb[A]) : 0.0;
-        }
-        if (model == GW_MODEL_J2) rm_j2<AD, double, AD>(etr, lam, mu, c.mc.kappa, e);
-        else if (model == GW_MODEL_DP) rm_dp<AD, double, AD>(etr, lam, mu, c.mc, e);
-        else for (int A = 0; A < 3; ++A) e[A] = etr[A];
-        tau_hencky(e, lam, mu, tA);
-        // coalescence limits from the value-level algorithmic tangent
-        double tv[3], dtau[3][4], ev[3], de[3][4], pn = 0.0;
-        principal_model<double, MODEL>(c.mc, lam.v, mu.v, etr_v, 0.0, 0.0, pn, tv, dtau, ev, true, de);
-        double limT[3][3], limB[3][3];
-        AD fB[3];
-        for (int A = 0; A < 3; ++A) {
-            fB[A] = gexp(e[A] * 2.0);
-            for (int Bq = 0; Bq < 3; ++Bq) {
-                limT[A][Bq] = (dtau[A][A] - dtau[A][Bq]) / (2.0 * lamb[A]);
-                limB[A][Bq] = 2.0 * fB[A].v * (de[A][A] - de[A][Bq]) / (2.0 * lamb[A]);
-            }
-        }
-        spectral_assemble(V, lamb, tA, limT, dbp, tau);
+        apply_cjac(cj.tv, cj.Jt, btr, E, tau);
         if (want_g2p) {  // b_new is a G2P output
             AD bn[3][3];
-            spectral_assemble(V, lamb, fB, limB, dbp, bn);
+            apply_cjac(cj.bv, cj.Jb, btr, E, bn);
             for (int i = 0; i < 3; ++i)
                 for (int j = 0; j < 3; ++j) o.s += bn[i][j] * wt.b[i * 3 + j];
         }
@@ -327,6 +431,32 @@ __device__ __forceinline__ void gather_du(const LaunchConst &c, const PtrsP &p, 
     }
 }
 
+// Trial left Cauchy-Green tensor f b_old f^T of the particle (values), with
+// f = I + H and H = sum_a du_a (x) grad N_a over the slots inside the grid:
+// the value part of the passes' kinematics.
+__device__ __forceinline__ void trial_b(const LaunchConst &c, const double *xv, const double *lpv,
+                                        const double *bo_v, const double du[9][2], double B[3][3]) {
+    const gw_grid_t &g = c.g;
+    Axis ax[2];
+    for (int k = 0; k < 2; ++k) gimp_axis(xv[k], lpv[k], g.h[k], g.inv_h[k], ax[k]);
+    double H[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int a = 0; a < 9; ++a) {
+        const int i = a % 3, j = a / 3;
+        const int cx = ax[0].lower + i, cy = ax[1].lower + j;
+        if (!(cx >= 0 && cx <= g.n_grid[0] && cy >= 0 && cy <= g.n_grid[1])) continue;
+        const double G0 = ax[0].gw[i] * ax[1].w[j], G1 = ax[0].w[i] * ax[1].gw[j];
+        for (int l = 0; l < 2; ++l) {
+            H[0][l] += G0 * du[a][l];
+            H[1][l] += G1 * du[a][l];
+        }
+    }
+    double f[3][3] = {{1.0 + H[0][0], H[0][1], 0.0}, {H[1][0], 1.0 + H[1][1], 0.0}, {0.0, 0.0, 1.0}};
+    double bo[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) bo[i][j] = bo_v[i * 3 + j];
+    congruence3(f, bo, B);
+}
+
 // Runs the chunked passes over inputs [0, n_inputs): q[i] = ds / d input_i.
 template <int MODEL>
 __device__ __forceinline__ void adjoint_passes(const LaunchConst &c, const PtrsP &p, int pid, const double du[9][2],
@@ -336,9 +466,17 @@ __device__ __forceinline__ void adjoint_passes(const LaunchConst &c, const PtrsP
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
     const bool ext = p.ext_flag && p.ext_flag[pid];
     const double fext[2] = {ext ? c.st.point_load[0] * ramp : 0.0, ext ? c.st.point_load[1] * ramp : 0.0};
+    ConstJac cj;
+    const int model = MODEL >= 0 ? MODEL : c.mc.model;
+    if (model == GW_MODEL_HENCKY || model == GW_MODEL_J2 || model == GW_MODEL_DP) {
+        double B[3][3];
+        trial_b(c, p.x + pid * 2, p.lp + pid * 2, p.b_old + (size_t)pid * 9, du, B);
+        constitutive_jac<MODEL>(c, model, B, E, wt.x != nullptr, cj);
+    }
+#pragma unroll 1
     for (int off = 0; off < n_inputs; off += kAdjChunk) {
         solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E,
-                            fext, du, off, wt, o);
+                            fext, du, off, wt, cj, o);
 #pragma unroll
         for (int l = 0; l < kAdjChunk; ++l)
             if (off + l < kAdjInputs) q[off + l] = o.s.d[l];

@@ -177,7 +177,9 @@ static inline int guard_check(cudaStream_t s, const char *where) {
     GW_CUDA(cudaStreamSynchronize(s));
     if (site == 0) return GW_OK;
     const int zero = 0;
+    const long long zero_v = 0;
     GW_CUDA(cudaMemcpyToSymbolAsync(g_guard_site, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, s));
+    GW_CUDA(cudaMemcpyToSymbolAsync(g_guard_value, &zero_v, sizeof(long long), 0, cudaMemcpyHostToDevice, s));
     GW_CUDA(cudaStreamSynchronize(s));
     snprintf(g_msg, sizeof(g_msg), "%s: index guard failed in %s (value %lld)", where,
              (site > 0 && site < GS_COUNT) ? kGuardNames[site] : "unknown site", value);

@@ -39,7 +39,7 @@ extern "C" {
 #define GW_ENOCONV -3       /* Krylov iteration cap reached before tolerance     */
 #define GW_EBREAKDOWN -4    /* Krylov breakdown (rho or omega underflow)         */
 #define GW_ENAN -5          /* non-finite value detected                         */
-#define GW_ERANGE -6        /* particle support left the grid                    */
+#define GW_ERANGE -6        /* a device index guard failed (see gw_guard_read)   */
 #define GW_EMODEL -7        /* unknown material model for this solver kind       */
 
 /* ------------------------------------------------------------ enums */

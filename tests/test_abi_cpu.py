@@ -30,7 +30,7 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(lib, name), name
         assert name in _lib.SIGNATURES, name
     assert lib.gw_version() == 1
-    assert lib.gw_status_string(-6).decode().startswith("particle support")
+    assert lib.gw_status_string(-6).decode().startswith("index guard")
 
 
 def test_struct_layouts_match_c():
