@@ -323,6 +323,12 @@ extern "C" int gw_tune_set(int32_t knob, int32_t value) {
         case GW_TUNE_MG_OMEGA:
             if (value < 10 || value > 100) return GW_EINVAL;
             break;
+        case GW_TUNE_GS_CANCEL:
+            if (value < 0 || value > 300) return GW_EINVAL;
+            break;
+        case GW_TUNE_MG_TAIL:
+            if (value < 0 || value > (1 << 20)) return GW_EINVAL;
+            break;
         default:
             return GW_EINVAL;
     }

@@ -5,6 +5,7 @@
 
 #include "gw_host.cuh"
 #include "gw_mg.cuh"
+#include "gw_mg_tail.cuh"
 
 using namespace gw;
 using namespace gwh;
@@ -100,6 +101,20 @@ int krylov_nf(const gw_bsr_t *A, int method, int precond, const double *b, doubl
 }  // namespace
 
 namespace {
+// second Gram-Schmidt passes of the last GMRES solve on this host thread
+thread_local int g_last_reorths = 0;
+
+// Profiling only: whether column k takes the second Gram-Schmidt pass (read
+// after pass 0), so that the timed pass-1 launches are credited with the bytes
+// they move.  Timed runs without profiling never read it.
+int prof_reorth(GScalars *sc, cudaStream_t s) {
+    if (!g_prof_on) return 1;
+    int re = 1;
+    if (cudaMemcpyAsync(&re, &sc->reorth, sizeof(int), cudaMemcpyDeviceToHost, s) != cudaSuccess) return 1;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
+    return re;
+}
+
 int64_t gmres_ws_bytes(int64_t n_rows, int nf, int restart) {
     const int64_t n = n_rows * nf;
     return align256(8 * n * (restart + 1)) + 2 * align256(8 * n) + align256(8 * n_rows * nf * nf) +
@@ -126,6 +141,8 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
     GW_CUDA(cudaMemsetAsync(G.sc, 0, head, s));
     struct { int max_iter, restart; } lim = {max_iter, restart};
     GW_CUDA(cudaMemcpyAsync(&G.sc->max_iter, &lim, sizeof(lim), cudaMemcpyHostToDevice, s));
+    const double eta2 = ::pow(10.0, -0.1 * g_tune[GW_TUNE_GS_CANCEL]);
+    GW_CUDA(cudaMemcpyAsync(&G.sc->gs_eta2, &eta2, sizeof(double), cudaMemcpyHostToDevice, s));
     const int D = (A->mask_words == 1) ? 2 : 3;
     k_precond_setup<NF, VT><<<gw_count_launch(nblk(nr, kThreads)), kThreads, 0, s>>>(a, D, precond, G.Minv);
     GW_LAUNCHED();
@@ -148,10 +165,11 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
             for (int it = 0; it < chunk; ++it, ++kk) {
                 const double vb = 8.0 * n * (kk + 2);
                 { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
+                { ProfScope ps(PC_DOTS, s, vb + 8.0 * n); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
                 { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                const int re = prof_reorth(G.sc, s);
+                { ProfScope ps(PC_DOTS, s, re ? vb : 0.0); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_UPDATE, s, re ? vb + 8.0 * n : 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
                 { ProfScope ps(PC_NEXT, s, 8.0 * n * 3 + 8.0 * nr * NF * NF); k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 0); }
             }
             GW_LAUNCHED();
@@ -166,6 +184,7 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
         GW_LAUNCHED();
     }
     *iters = h.iters;
+    g_last_reorths = h.reorths;
     *relres = (h.bnorm > 0.0) ? h.resid / h.bnorm : 0.0;
     const int gc = guard_check(s, "GMRES");
     if (gc) return gc;
@@ -487,14 +506,124 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
     else k_mg_jacobi<NF, double><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
 }
 
+// Largest cluster of the fused coarse tail for this instantiation on the
+// current device: 16 CTAs where the device can run such a cluster of it, else
+// 8, 0 when neither fits (then every level keeps its own launches).  Queried once
+// per device, before any stream capture (gmres_mg calls it first).
+template <int D, int NF>
+int tail_cluster_size() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    if (cached[dev]) return cached[dev] > 0 ? cached[dev] : 0;
+    int size = -1;
+    for (int cand : {16, 8}) {
+        if (cand > 8 && cudaFuncSetAttribute(k_mg_tail<D, NF>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                            cudaSuccess)
+            continue;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cand);
+        cfg.blockDim = dim3(kTailThreads);
+        cudaLaunchAttribute at;
+        at.id = cudaLaunchAttributeClusterDimension;
+        at.val.clusterDim.x = cand;
+        at.val.clusterDim.y = 1;
+        at.val.clusterDim.z = 1;
+        cfg.attrs = &at;
+        cfg.numAttrs = 1;
+        int n = 0;
+        if (cudaOccupancyMaxActiveClusters(&n, (void *)k_mg_tail<D, NF>, &cfg) == cudaSuccess && n >= 1) {
+            size = cand;
+            break;
+        }
+    }
+    (void)cudaGetLastError();  // a refused query leaves no error behind
+    cached[dev] = size;
+    return size > 0 ? size : 0;
+}
+
+template <int NF>
+int tail_cluster_size(int D) { return D == 2 ? tail_cluster_size<2, NF>() : tail_cluster_size<3, NF>(); }
+
+// First level of the fused coarse tail (the first coarse level with at most
+// GW_TUNE_MG_TAIL rows), or h.nl - 1 when the tail is off or has no level to
+// smooth.
+template <int NF>
+int tail_level(const MgHier &h) {
+    const int last = h.nl - 1, T = g_tune[GW_TUNE_MG_TAIL];
+    if (T <= 0 || last < 2 || tail_cluster_size<NF>(h.lv[0].g.dim) == 0) return last;
+    for (int l = 1; l < last; ++l)
+        if (h.lv[l].A.n_rows <= T) return l;
+    return last;
+}
+
+// Launches levels l0 .. last of the V-cycle as one cluster and returns the
+// buffer that holds level l0's result (the same one the per-phase path ends in).
+template <int NF>
+double *mg_tail(const MgHier &h, int l0, const int *skip, cudaStream_t s) {
+    const int last = h.nl - 1, D = h.lv[0].g.dim;
+    TailArgs ta;
+    memset(&ta, 0, sizeof(ta));
+    ta.l0 = l0;
+    ta.last = last;
+    ta.dInv = h.dInv;
+    ta.dn = h.dn;
+    ta.omega = mg_omega();
+    ta.skip = skip;
+    double bytes = 8.0 * h.dn * h.dn;
+    for (int l = l0; l <= last; ++l) {
+        const MgLevel &v = h.lv[l];
+        TailLevel &t = ta.lv[l];
+        t.A = make_ptrs(v.A);
+        t.L = v.L;
+        t.Minv = v.Minv;
+        t.b = v.b; t.x = v.x; t.x2 = v.x2; t.r = v.r;
+        t.fixed = v.fixed;
+        t.sweeps = mg_sweeps(l);
+        if (l < last) {
+            const double vs = 8.0 * v.A.n_rows * NF, vc = 8.0 * h.lv[l + 1].A.n_rows * NF;
+            const double mat = (double)v.A.nnzb * (NF * NF * 8 + 4), minv = 8.0 * v.A.n_rows * NF * NF;
+            bytes += (mat + 2 * vs + minv) + (mat + 3 * vs) + (vs + vc) + (2 * vs + vc) + t.sweeps * (mat + 3 * vs + minv);
+        }
+    }
+    // cluster just large enough for two block rows of level l0 per row group
+    // (128 groups per CTA), at most what the device runs
+    const int cmax = tail_cluster_size<NF>(D), need = (h.lv[l0].A.n_rows + 255) / 256;
+    int cl = 1;
+    while (cl < need && cl < cmax) cl *= 2;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl);
+    cfg.blockDim = dim3(kTailThreads);
+    cfg.stream = s;
+    cudaLaunchAttribute at;
+    at.id = cudaLaunchAttributeClusterDimension;
+    at.val.clusterDim.x = cl;
+    at.val.clusterDim.y = 1;
+    at.val.clusterDim.z = 1;
+    cfg.attrs = &at;
+    cfg.numAttrs = 1;
+    {
+        ProfScope ps(PC_MG_TAIL, s, bytes);
+        gw_count_launch(cl);
+        if (D == 2) cudaLaunchKernelEx(&cfg, k_mg_tail<2, NF>, ta);
+        else cudaLaunchKernelEx(&cfg, k_mg_tail<3, NF>, ta);
+    }
+    // the buffer the per-phase path would end level l0 in: x on the way down,
+    // alternating with x2 once per sweep
+    const int S = mg_sweeps(l0);
+    const int swaps = (S >= 2 ? 1 + (S - 2) : S - 1) + S;
+    return (swaps & 1) ? h.lv[l0].x2 : h.lv[l0].x;
+}
+
 // One V-cycle on h.lv[0].b; returns the buffer that holds the result (the same
-// buffer on every call).
+// buffer on every call).  Levels from tail_level() down run fused (mg_tail).
 template <int NF, typename VT>
 double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
     const int last = h.nl - 1;
     const int D = h.lv[0].g.dim;
+    const int l0 = tail_level<NF>(h);
     double *cur[kMgMaxLevels], *oth[kMgMaxLevels];
-    for (int l = 0; l < last; ++l) {
+    for (int l = 0; l < l0; ++l) {
         const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
         double *x = v.x, *y = v.x2;
         if (mg_sweeps(l) >= 2) {
@@ -535,10 +664,14 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         cur[l] = x;
         oth[l] = y;
     }
-    const MgLevel &lc = h.lv[last];
-    k_mg_dense_apply<<<gw_count_launch(nblk((int64_t)h.dn * 32, kThreads)), kThreads, 0, s>>>(h.dInv, lc.b, lc.x, h.dn, skip);
-    cur[last] = lc.x;
-    for (int l = last - 1; l >= 0; --l) {
+    if (l0 < last) {
+        cur[l0] = mg_tail<NF>(h, l0, skip, s);
+    } else {
+        const MgLevel &lc = h.lv[last];
+        k_mg_dense_apply<<<gw_count_launch(nblk((int64_t)h.dn * 32, kThreads)), kThreads, 0, s>>>(h.dInv, lc.b, lc.x, h.dn, skip);
+        cur[last] = lc.x;
+    }
+    for (int l = l0 - 1; l >= 0; --l) {
         const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
         PtrsA a = make_ptrs(v.A), ca = make_ptrs(c.A);
         double *x = cur[l], *y = oth[l];
@@ -563,7 +696,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
 // instantiated graph serves all Newton iterations of a load step.  The graphs
 // are held in a small cache (least recently used entry replaced).
 struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega;
+    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega, tail;
     int n_grid[3];
     int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
     gw_bsr_t A;
@@ -616,6 +749,7 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
     k.one_sweep = g_tune[GW_TUNE_MG_ONE_SWEEP];
     k.sweeps = g_tune[GW_TUNE_MG_SWEEPS];
     k.omega = g_tune[GW_TUNE_MG_OMEGA];
+    k.tail = g_tune[GW_TUNE_MG_TAIL];
     for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
     for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
     k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;
@@ -667,6 +801,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
     const int nr = A->n_rows;
     if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
     const int64_t n = (int64_t)nr * NF;
+    (void)tail_cluster_size<NF>(grid->dim);  // device query before any stream capture
     Bump bp{(char *)ws, 0};
     MgHier h;
     FlexVecs fv;
@@ -708,6 +843,8 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
     GW_CUDA(cudaMemsetAsync(G.sc, 0, head, s));
     struct { int max_iter, restart; } lim = {max_iter, restart};
     GW_CUDA(cudaMemcpyAsync(&G.sc->max_iter, &lim, sizeof(lim), cudaMemcpyHostToDevice, s));
+    const double eta2 = ::pow(10.0, -0.1 * g_tune[GW_TUNE_GS_CANCEL]);
+    GW_CUDA(cudaMemcpyAsync(&G.sc->gs_eta2, &eta2, sizeof(double), cudaMemcpyHostToDevice, s));
     const int gr = red_grid_rows(nr), gv = red_grid_elems(n);
     const int *skip = &G.sc->cycle_done;
     GScalars hs;
@@ -748,10 +885,11 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
                 }
                 const double vb = 8.0 * n * (kk + 2);
                 { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv_keep<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, fv.Z); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
+                { ProfScope ps(PC_DOTS, s, vb + 8.0 * n); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
                 { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
-                { ProfScope ps(PC_DOTS, s, vb); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                const int re = prof_reorth(G.sc, s);
+                { ProfScope ps(PC_DOTS, s, re ? vb : 0.0); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_UPDATE, s, re ? vb + 8.0 * n : 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
                 { ProfScope ps(PC_NEXT, s, 8.0 * n * 3); k_gm_next_flex<<<gw_count_launch(gv), kThreads, 0, s>>>((size_t)n, G, 0, h.lv[0].b); }
                 mg_vcycle<NF, VT>(h, skip, s);
             }
@@ -775,6 +913,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
         GW_LAUNCHED();
     }
     *iters = hs.iters;
+    g_last_reorths = hs.reorths;
     *relres = (hs.bnorm > 0.0) ? hs.resid / hs.bnorm : 0.0;
     if (plan_in) plan_in->last_iters = hs.iters;
     rc = guard_check(s, "multigrid GMRES");
@@ -837,6 +976,8 @@ extern "C" int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *
     plan_host->workspace = workspace;
     return GW_OK;
 }
+
+extern "C" int32_t gw_gmres_last_reorths(void) { return g_last_reorths; }
 
 extern "C" int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec,
                                      gw_mg_plan_t *plan_host, const double *b, double *x, double rtol,

@@ -43,12 +43,12 @@ static inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
 // algorithmic bytes the host attributed to each launch.
 enum ProfClass {
     PC_ASSEMBLE = 0, PC_SPMV, PC_DOTS, PC_UPDATE, PC_NEXT, PC_G2P, PC_ADJ_G2P, PC_ADJ_RES,
-    PC_MG_JACOBI, PC_MG_RESID, PC_MG_TRANSFER, PC_MG_SETUP, PC_MG_JACOBI_COARSE, PC_COUNT
+    PC_MG_JACOBI, PC_MG_RESID, PC_MG_TRANSFER, PC_MG_SETUP, PC_MG_JACOBI_COARSE, PC_MG_TAIL, PC_COUNT
 };
 inline const char *kProfNames[PC_COUNT] = {"k_assemble", "k_gm_spmv", "k_gm_dots", "k_gm_update", "k_gm_next", "k_g2p",
                                     "k_adjoint_g2p", "k_adjoint_residual", "k_mg_jacobi (finest level)",
                                     "k_mg_residual", "k_mg_restrict/prolong", "mg_setup",
-                                    "k_mg_jacobi (coarse levels)"};
+                                    "k_mg_jacobi (coarse levels)", "k_mg_tail (fused coarse levels)"};
 struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
 inline bool g_prof_on = false;
 inline ProfRec *g_prof = nullptr;
@@ -97,7 +97,7 @@ static inline bool vec_ok(const gw_bsr_t *A, const void *u, const void *v) {
 
 // launch-shape knobs (gw_tune_set): particle CTA, adjoint CTA, warps per CTA
 // of the multigrid row kernels, bound of the dense coarsest level
-inline int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160, GW_MG_MAX_LEVELS, 2, 70};
+inline int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160, GW_MG_MAX_LEVELS, 2, 70, 20, 0};
 // block-row kernels: kRowsPerWarp rows per warp (groups of kLPR lanes)
 static inline int tune_rows_grid(int n_rows) {
     const int w = g_tune[GW_TUNE_ROW_WARPS];

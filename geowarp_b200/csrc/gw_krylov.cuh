@@ -564,15 +564,23 @@ namespace gw {
 namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 // ---------------------------------------------------------------- restarted GMRES(m)
-// Right-preconditioned GMRES with classical Gram-Schmidt and one
-// re-orthogonalisation pass.  Column k of the Arnoldi process is six kernels:
+// Right-preconditioned GMRES with classical Gram-Schmidt and a
+// re-orthogonalisation pass when needed.  Column k of the Arnoldi process is
+// six kernels:
 //   spmv:  w = A z_k                       (z_k = Minv v_k)
-//   dots:  h_i = (v_i, w), i <= k          (pass 0)
+//   dots:  h_i = (v_i, w), i <= k, and (w, w)   (pass 0); the last block
+//          decides the second pass: ||w - V h||^2 = (w, w) - sum h_i^2 below
+//          gs_eta2 (w, w) (by default 1/100: the projection removed more than
+//          90% of w's norm) means V h lost more than ~10 ulp of orthogonality
+//          and the pass is repeated
 //   upd:   w -= V h                        (pass 0)
-//   dots:  h2_i = (v_i, w)                 (pass 1)
-//   upd:   w -= V h2 ; ||w||; last block: Hessenberg column, Givens rotation,
-//          residual estimate, cycle/convergence flags, k += 1
+//   dots:  h2_i = (v_i, w)                 (pass 1, only when needed)
+//   upd:   w -= V h2 (only when needed) ; ||w||; last block: Hessenberg
+//          column, Givens rotation, residual estimate, cycle/convergence
+//          flags, k += 1
 //   next:  v_k = w / ||w|| ; z_k = Minv v_k
+// The skipped pass reads no basis vector, so an Arnoldi step without strong
+// cancellation reads the basis twice instead of four times.
 // Robust for the nonsymmetric, indefinite Jacobians of the penalty footing
 // and the u-p saddle-point systems, on which BiCGSTAB breaks down.
 constexpr int kGmresMaxRestart = 128;
@@ -580,9 +588,12 @@ constexpr int kGmresMaxRestart = 128;
 struct GScalars {
     // scalar header first: the host polls only this prefix
     double beta, bnorm, tol, resid, wnorm;
+    double gs_eta2;  // second Gram-Schmidt pass below this fraction of ||w||^2 left
     int k;           // completed Arnoldi columns in the current cycle
     int cycle_done, done, status, iters, max_iter, restart;
     unsigned ticket;
+    int reorth;      // column k takes the second Gram-Schmidt pass
+    int reorths;     // second passes taken in this solve
     double H[kGmresMaxRestart + 1][kGmresMaxRestart];
     double cs[kGmresMaxRestart], sn[kGmresMaxRestart];
     double g[kGmresMaxRestart + 1];
@@ -670,18 +681,22 @@ __global__ void k_gm_spmv(PtrsA A, GmresVecs G) {
 }
 
 // (v_i, w) for i <= k; block partials reduced in block order by the last block
+// (pass 0 also (w, w) as item k + 1, and the decision on pass 1)
 __global__ void k_gm_dots(GmresVecs G, int pass) {
     if (G.sc->cycle_done) return;
+    if (pass == 1 && !G.sc->reorth) return;  // uniform over the grid
     const int k = G.sc->k;
     if (!in_range(k, G.sc->restart, GS_KRYLOV_K)) return;  // uniform over the grid: no block takes the ticket
+    const int m = pass == 0 ? k + 1 : k;                     // last item (k < restart <= kGmresMaxRestart)
     const size_t n = G.n;
     __shared__ double sh[kGmresMaxRestart + 1];
+    __shared__ double wsq;
     __shared__ bool last;
     const size_t per = (n + gridDim.x - 1) / gridDim.x;
     const size_t r0 = (size_t)blockIdx.x * per, r1 = min(n, r0 + per);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int i = warp; i <= k; i += nwarp) {
-        const double *vi = G.V + (size_t)i * n;
+    for (int i = warp; i <= m; i += nwarp) {
+        const double *vi = i <= k ? G.V + (size_t)i * n : G.w;
         double s = 0.0;
         for (size_t q = r0 + lane; q < r1; q += 32) s += vi[q] * G.w[q];
 #pragma unroll
@@ -689,7 +704,7 @@ __global__ void k_gm_dots(GmresVecs G, int pass) {
         if (lane == 0) sh[i] = s;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i <= k; i += blockDim.x) G.partials[(size_t)blockIdx.x * (kGmresMaxRestart + 1) + i] = sh[i];
+    for (int i = threadIdx.x; i <= m; i += blockDim.x) G.partials[(size_t)blockIdx.x * (kGmresMaxRestart + 1) + i] = sh[i];
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -700,19 +715,29 @@ __global__ void k_gm_dots(GmresVecs G, int pass) {
     __threadfence();
     // one warp per basis vector: lanes take the block partials in a fixed
     // stride, then a fixed shuffle tree (deterministic)
-    for (int i = warp; i <= k; i += nwarp) {
+    for (int i = warp; i <= m; i += nwarp) {
         double s = 0.0;
         for (int bb = lane; bb < (int)gridDim.x; bb += 32)
             s += ((volatile double *)G.partials)[(size_t)bb * (kGmresMaxRestart + 1) + i];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
         if (lane == 0) {
-            if (pass == 0) G.sc->H[i][k] = s;
+            if (i > k) wsq = s;
+            else if (pass == 0) G.sc->H[i][k] = s;
             else G.sc->h2[i] = s;
         }
     }
     __syncthreads();
-    if (threadIdx.x == 0) G.sc->ticket = 0u;
+    if (threadIdx.x == 0) {
+        if (pass == 0) {
+            double rem = wsq;
+            for (int i = 0; i <= k; ++i) rem -= G.sc->H[i][k] * G.sc->H[i][k];
+            const int re = !(rem >= G.sc->gs_eta2 * wsq);  // also when rem or wsq is not finite
+            G.sc->reorth = re;
+            G.sc->reorths += re;
+        }
+        G.sc->ticket = 0u;
+    }
 }
 
 // w -= V c (c = H[.][k] on pass 0, h2 on pass 1); pass 1 closes column k
@@ -722,19 +747,28 @@ __global__ void k_gm_update(GmresVecs G, int pass) {
     const int k = sc->k;
     if (!in_range(k, sc->restart, GS_KRYLOV_K)) return;  // uniform over the grid
     const size_t n = G.n;
+    const bool second = pass == 1 && sc->reorth;  // uniform over the grid
     __shared__ double coef[kGmresMaxRestart + 1];
     for (int i = threadIdx.x; i <= k; i += blockDim.x) coef[i] = pass == 0 ? sc->H[i][k] : sc->h2[i];
     __syncthreads();
     double d[1] = {0.0};
-    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-        double w = G.w[q];
-        for (int i = 0; i <= k; ++i) w -= coef[i] * G.V[(size_t)i * n + q];
-        G.w[q] = w;
-        d[0] += w * w;
+    if (pass == 0 || second) {
+        for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+            double w = G.w[q];
+            for (int i = 0; i <= k; ++i) w -= coef[i] * G.V[(size_t)i * n + q];
+            G.w[q] = w;
+            d[0] += w * w;
+        }
+    } else {  // no second pass: the norm only
+        for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+            const double w = G.w[q];
+            d[0] += w * w;
+        }
     }
     if (pass == 0) return;
     if (grid_reduce<1>(d, G.partials, &sc->ticket) && threadIdx.x == 0) {
-        for (int i = 0; i <= k; ++i) sc->H[i][k] += sc->h2[i];
+        if (second)
+            for (int i = 0; i <= k; ++i) sc->H[i][k] += sc->h2[i];
         const double hn = ::sqrt(d[0]);
         sc->wnorm = hn;
         sc->H[k + 1][k] = hn;

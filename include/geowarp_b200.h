@@ -359,6 +359,12 @@ int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *workspace, 
 int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec, gw_mg_plan_t *plan_host,
                           const double *b, double *x, double rtol, int32_t max_iter, int32_t restart, void *workspace,
                           int64_t workspace_bytes, int32_t *iters_host, double *relres_host, void *stream);
+/* Second (re-orthogonalisation) Gram-Schmidt passes taken by the last
+ * gw_bsr_gmres_solve / gw_bsr_gmres_mg_solve on the calling host thread.
+ * Both solvers project each new Krylov vector once and repeat the projection
+ * only when it cancelled more of the vector's norm than GW_TUNE_GS_CANCEL
+ * allows. */
+int32_t gw_gmres_last_reorths(void);
 /* y = A x (x, y FP64 of length n_rows*nf; A values in prec). */
 int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream);
 /* y = A^T x. */
@@ -453,8 +459,28 @@ const char *gw_profile_name(int32_t cls);
  *                           correction on the other levels, 1..4 (default 2)
  *   GW_TUNE_MG_OMEGA        damping of those sweeps in percent, 10..100
  *                           (default 70)
- * The last two change the preconditioner (Krylov iteration counts), not the
- * solution GMRES converges to; they also recapture the step graphs.
+ *   GW_TUNE_GS_CANCEL       GMRES Gram-Schmidt: a second projection pass is
+ *                           taken when the first left less than
+ *                           10^(-value/10) of the new vector's squared norm,
+ *                           0..300 (default 20: below 1/100, i.e. the
+ *                           projection removed more than 90% of the norm,
+ *                           so a column loses at most ~10 ulp of
+ *                           orthogonality; 3: the classical 1/2; 0: always;
+ *                           300: never unless non-finite)
+ *   GW_TUNE_MG_TAIL         most block rows of a multigrid level run by the
+ *                           fused coarse tail: that level and every coarser
+ *                           one go through one launch of one thread-block
+ *                           cluster with cluster barriers between the
+ *                           phases (bitwise the same V-cycle; the cluster
+ *                           has 1 to 16 CTAs, two rows of the first tail
+ *                           level per 8-lane group), 0..1048576 (default 0:
+ *                           one launch per phase); recaptures the step
+ *                           graphs.  It pays where the levels are a few
+ *                           hundred rows (launch-bound hierarchies)
+ * MG_SWEEPS and MG_OMEGA change the preconditioner (Krylov iteration counts),
+ * not the solution GMRES converges to; they also recapture the step graphs.
+ * GS_CANCEL changes the orthogonality of the Krylov basis and so the
+ * iteration count and the attainable accuracy; it is read at each solve.
  * gw_tune_set returns GW_EINVAL outside these ranges; gw_tune_get returns -1
  * for an unknown knob. */
 #define GW_TUNE_PARTICLE_BLOCK 0
@@ -464,7 +490,9 @@ const char *gw_profile_name(int32_t cls);
 #define GW_TUNE_MG_ONE_SWEEP 4
 #define GW_TUNE_MG_SWEEPS 5
 #define GW_TUNE_MG_OMEGA 6
-#define GW_TUNE_COUNT 7
+#define GW_TUNE_GS_CANCEL 7
+#define GW_TUNE_MG_TAIL 8
+#define GW_TUNE_COUNT 9
 int gw_tune_set(int32_t knob, int32_t value);
 int32_t gw_tune_get(int32_t knob);
 

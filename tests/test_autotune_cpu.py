@@ -7,7 +7,8 @@ from geowarp_b200 import _lib as L
 from geowarp_b200 import autotune
 
 DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160,
-            L.TUNE_MG_ONE_SWEEP: 20, L.TUNE_MG_SWEEPS: 2, L.TUNE_MG_OMEGA: 70}
+            L.TUNE_MG_ONE_SWEEP: 20, L.TUNE_MG_SWEEPS: 2, L.TUNE_MG_OMEGA: 70, L.TUNE_GS_CANCEL: 20,
+            L.TUNE_MG_TAIL: 0}
 
 
 @pytest.fixture
@@ -25,6 +26,7 @@ def test_knob_defaults_and_ranges(lib):
     bad = [(L.TUNE_PARTICLE_BLOCK, 288), (L.TUNE_PARTICLE_BLOCK, 48), (L.TUNE_ADJOINT_BLOCK, 0),
            (L.TUNE_ROW_WARPS, 0), (L.TUNE_ROW_WARPS, 33), (L.TUNE_MG_COARSE, 7), (L.TUNE_MG_COARSE, 161),
            (L.TUNE_MG_ONE_SWEEP, 0), (L.TUNE_MG_ONE_SWEEP, 21), (L.TUNE_MG_SWEEPS, 5), (L.TUNE_MG_OMEGA, 101),
+           (L.TUNE_GS_CANCEL, -1), (L.TUNE_GS_CANCEL, 301), (L.TUNE_MG_TAIL, -1), (L.TUNE_MG_TAIL, (1 << 20) + 1),
            (L.TUNE_COUNT, 1)]
     for k, v in bad:
         assert lib.gw_tune_set(k, v) == L.GW_EINVAL, (k, v)
@@ -37,11 +39,11 @@ def test_knob_defaults_and_ranges(lib):
 
 
 def test_coordinate_search_finds_the_separable_optimum(lib):
-    target = {"row_warps": 4, "mg_coarse": 80, "particle_block": 128, "adjoint_block": 64}
+    target = {"row_warps": 4, "mg_coarse": 80, "mg_tail": 512, "particle_block": 128, "adjoint_block": 64}
 
     def cost():
         cfg = autotune.current()
-        return sum((cfg[n] - target[n]) ** 2 / float(target[n]) for n in target) + 1.0
+        return sum((cfg[n] - target[n]) ** 2 / float(target[n] or 1) for n in target) + 1.0
 
     calls = []
     best, table = autotune.tune(lambda: calls.append(1), reps=3, timer=lambda fn: (fn(), cost())[1])

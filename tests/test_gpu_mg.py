@@ -70,8 +70,11 @@ def _true_relres(e, x):
 def test_mg_gmres_matches_jacobi_gmres_on_bar(cuda, precision):
     s, step = _system_bar(precision)
     e = _assembled(s, step)
+    from geowarp_b200 import _lib as L
     x_j, it_j, rr_j, rc_j = _solve(e, "block", 1e-12)
     x_m, it_m, rr_m, rc_m = _solve(e, "mg", 1e-12)
+    # second Gram-Schmidt passes are taken only where the projection cancelled
+    assert 0 <= L.load().gw_gmres_last_reorths() <= it_m
     assert rc_j == 0 and rc_m == 0
     assert _true_relres(e, x_m) < 1e-10
     assert rel_err(x_m.cpu().numpy(), x_j.cpu().numpy()) < 1e-9
@@ -205,3 +208,27 @@ def test_launch_knobs_change_speed_not_results(cuda):
             lib.gw_tune_set(k, v)
     assert rel_err(u1, u0) < 1e-9
     assert rel_err(g1, g0) < 1e-7
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_coarse_tail_is_bitwise_the_per_phase_vcycle(cuda, precision):
+    """The coarse levels run as one cluster launch (GW_TUNE_MG_TAIL) give the
+    same bytes as one launch per phase, in fewer launches."""
+    from geowarp_b200 import _lib as L
+    lib = L.load()
+    default = lib.gw_tune_get(L.TUNE_MG_TAIL)
+    s, step = _system_footing(precision)
+    e = _assembled(s, step)
+    out = {}
+    try:
+        for tail in (0, 4096):
+            assert lib.gw_tune_set(L.TUNE_MG_TAIL, tail) == L.GW_OK
+            n0 = lib.gw_launch_count()
+            x, it, rr, rc = _solve(e, "mg", 1e-10)
+            out[tail] = (x.cpu().numpy(), it, rc, lib.gw_launch_count() - n0)
+    finally:
+        lib.gw_tune_set(L.TUNE_MG_TAIL, default)
+    (x0, it0, rc0, n_sep), (x1, it1, rc1, n_tail) = out[0], out[4096]
+    assert rc0 == 0 and rc1 == 0 and it0 == it1
+    assert np.array_equal(x0, x1)
+    assert n_tail < n_sep
