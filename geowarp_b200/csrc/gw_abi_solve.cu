@@ -256,6 +256,8 @@ struct MgLevel {
     double *Minv, *b, *x, *x2, *r;
     uint8_t *fixed;
     int *tmp, *sws, *blockrow;
+    int *child;             // coarse levels: fine rows of the 3^D children of each row (pattern phase)
+    int *parent;            // levels with a coarser one: coarse rows of the 2^D parents of each row
     uint8_t *flags;
 };
 struct MgHier {
@@ -303,6 +305,8 @@ void mg_carve_hier(Bump &bp, MgHier &h, const gw_grid_t &g0, int64_t n_rows0, in
     l0.x2 = (double *)bp.take(8 * n0);
     l0.r = (double *)bp.take(8 * n0);
     l0.fixed = (uint8_t *)bp.take(n_rows0);
+    const int CN = D == 2 ? 9 : 27, PN = D == 2 ? 4 : 8;
+    l0.parent = (int *)bp.take(4 * n_rows0 * PN);
     gw_grid_t g = g0;
     int64_t nodes = g0.n_nodes;
     int l = 0;
@@ -328,6 +332,8 @@ void mg_carve_hier(Bump &bp, MgHier &h, const gw_grid_t &g0, int64_t n_rows0, in
         c.x2 = (double *)bp.take(8 * nodes * nf);
         c.r = (double *)bp.take(8 * nodes * nf);
         c.fixed = (uint8_t *)bp.take(nodes);
+        c.child = (int *)bp.take(4 * nodes * CN);
+        c.parent = (int *)bp.take(4 * nodes * PN);
     }
     h.nl = l + 1;  // upper bound; the plan may stop earlier
     h.dM = (double *)bp.take(8 * (int64_t)kMgCoarseMax * kMgCoarseMax);
@@ -409,6 +415,13 @@ int mg_pattern(MgHier &h, const gw_bsr_t *A0, gw_mg_plan_t *plan, cudaStream_t s
         if (D == 2) k_pattern_fill<2><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(c.g, ca, (int *)c.A.cols);
         else k_pattern_fill<3><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(c.g, ca, (int *)c.A.cols);
         k_mg_blockrow<<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(c.A.row_ptr, nrc, nnzb, c.blockrow);
+        if (D == 2) {
+            k_mg_children<2><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(f.L, fa, c.L, ca, c.child);
+            k_mg_parents<2><<<gw_count_launch(nblk(f.A.n_rows, kThreads)), kThreads, 0, s>>>(f.L, fa, c.L, ca, f.parent);
+        } else {
+            k_mg_children<3><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(f.L, fa, c.L, ca, c.child);
+            k_mg_parents<3><<<gw_count_launch(nblk(f.A.n_rows, kThreads)), kThreads, 0, s>>>(f.L, fa, c.L, ca, f.parent);
+        }
         GW_LAUNCHED();
         ++l;
     }
@@ -659,8 +672,12 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         else k_mg_residual<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
         }
         ProfScope ps(PC_MG_TRANSFER, s, vs + 8.0 * c.A.n_rows * NF);
-        if (D == 2) k_mg_restrict<2, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, v.r, c.b, skip);
-        else k_mg_restrict<3, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, v.r, c.b, skip);
+        if (D == 2)
+            k_mg_restrict_list<2, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(
+                c.A.n_rows, v.A.n_rows, c.child, v.fixed, v.r, c.b, skip);
+        else
+            k_mg_restrict_list<3, NF><<<gw_count_launch(nblk(c.A.n_rows, kThreads)), kThreads, 0, s>>>(
+                c.A.n_rows, v.A.n_rows, c.child, v.fixed, v.r, c.b, skip);
         cur[l] = x;
         oth[l] = y;
     }
@@ -677,8 +694,12 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         double *x = cur[l], *y = oth[l];
         {
         ProfScope ps(PC_MG_TRANSFER, s, 16.0 * v.A.n_rows * NF + 8.0 * c.A.n_rows * NF);
-        if (D == 2) k_mg_prolong<2, NF><<<gw_count_launch(nblk(v.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, cur[l + 1], x, skip);
-        else k_mg_prolong<3, NF><<<gw_count_launch(nblk(v.A.n_rows, kThreads)), kThreads, 0, s>>>(v.L, a, v.fixed, c.L, ca, cur[l + 1], x, skip);
+        if (D == 2)
+            k_mg_prolong_list<2, NF><<<gw_count_launch(nblk(v.A.n_rows, kThreads)), kThreads, 0, s>>>(
+                v.A.n_rows, c.A.n_rows, v.parent, v.fixed, cur[l + 1], x, skip);
+        else
+            k_mg_prolong_list<3, NF><<<gw_count_launch(nblk(v.A.n_rows, kThreads)), kThreads, 0, s>>>(
+                v.A.n_rows, c.A.n_rows, v.parent, v.fixed, cur[l + 1], x, skip);
         }
         for (int it = 0; it < mg_sweeps(l); ++it) {
             mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);

@@ -506,6 +506,144 @@ __global__ void k_mg_prolong(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixe
         if (!((fx >> f) & 1)) xf[(size_t)r * NF + f] += acc[f];
 }
 
+// ---------------------------------------------------------------- transfer lists
+// The transfers above find each child / parent through the lattice
+// (row2node, coordinates, node2row) on every V-cycle.  The pattern phase
+// resolves those lookups once per load step into row lists, so a V-cycle's
+// restriction and prolongation read an index list and then the vector: two
+// dependent loads instead of three per child.  The lists keep the loop order
+// of k_mg_restrict / k_mg_prolong, so the sums are bitwise the same.
+
+// child[R * 3^D + q]: fine row of child q (q = ox+1 + 3 (oy+1) [+ 9 (oz+1)]) of
+// coarse row R, -1 where the child is outside the lattice or inactive
+template <int D>
+__global__ void k_mg_children(Lat Lf, PtrsA Af, Lat Lc, PtrsA Ac, int *__restrict__ child) {
+    constexpr int CN = D == 2 ? 9 : 27;
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= Ac.n_rows) return;
+    int *out = child + (size_t)R * CN;
+    const int I = Ac.row2node[R];
+    if (!in_range(I, lat_size(Lc), GS_RESTRICT)) {
+        for (int q = 0; q < CN; ++q) out[q] = -1;
+        return;
+    }
+    int C[3];
+    lat_coords(Lc, I, C);
+    int q = 0;
+    for (int oz = (D == 3 ? -1 : 0); oz <= (D == 3 ? 1 : 0); ++oz)
+        for (int oy = -1; oy <= 1; ++oy)
+            for (int ox = -1; ox <= 1; ++ox, ++q) {
+                const int ci[3] = {2 * C[0] + ox, 2 * C[1] + oy, 2 * C[2] + oz};
+                bool in = true;
+                for (int k = 0; k < D; ++k) in = in && ci[k] >= 0 && ci[k] < Lf.n[k];
+                int fr = -1;
+                if (in) {
+                    fr = Af.node2row[lat_id(Lf, ci)];
+                    if (fr < 0 || !in_range(fr, Af.n_rows, GS_RESTRICT)) fr = -1;
+                }
+                out[q] = fr;
+            }
+}
+
+// parent[r * 2^D + q]: coarse rows of fine row r in k_mg_prolong's loop order,
+// -1 where that parent is outside the lattice or inactive, -2 past the
+// parity count (the weight of every parent is 1 / that count)
+template <int D>
+__global__ void k_mg_parents(Lat Lf, PtrsA Af, Lat Lc, PtrsA Ac, int *__restrict__ parent) {
+    constexpr int PN = D == 2 ? 4 : 8;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= Af.n_rows) return;
+    int *out = parent + (size_t)r * PN;
+    for (int q = 0; q < PN; ++q) out[q] = -2;
+    const int node = Af.row2node[r];
+    if (!in_range(node, lat_size(Lf), GS_PROLONG)) return;
+    int c[3];
+    lat_coords(Lf, node, c);
+    int lo[3], cnt[3];
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = c[k] >> 1;
+        cnt[k] = (k < D && (c[k] & 1)) ? 2 : 1;
+    }
+    int q = 0;
+    for (int a = 0; a < cnt[0]; ++a)
+        for (int b = 0; b < cnt[1]; ++b)
+            for (int d = 0; d < cnt[2]; ++d, ++q) {
+                const int C[3] = {lo[0] + a, lo[1] + b, lo[2] + d};
+                const int cid = lat_id(Lc, C);
+                int R = -1;
+                if (in_range(cid, lat_size(Lc), GS_PROLONG)) {
+                    R = Ac.node2row[cid];
+                    if (R < 0 || !in_range(R, Ac.n_rows, GS_PROLONG)) R = -1;
+                }
+                out[q] = R;
+            }
+}
+
+// b_c = P^T r_f through the child lists
+template <int D, int NF>
+__global__ void k_mg_restrict_list(int nc, int nf_rows, const int *__restrict__ child,
+                                   const uint8_t *__restrict__ ffixed, const double *__restrict__ rf,
+                                   double *__restrict__ bc, const int *__restrict__ skip) {
+    constexpr int CN = D == 2 ? 9 : 27;
+    if (skip && *skip) return;
+    const int R = blockIdx.x * blockDim.x + threadIdx.x;
+    if (R >= nc) return;
+    const int *ch = child + (size_t)R * CN;
+    int fr[CN];
+#pragma unroll
+    for (int q = 0; q < CN; ++q) fr[q] = ch[q];
+    double acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[f] = 0.0;
+#pragma unroll
+    for (int q = 0; q < CN; ++q) {
+        if (fr[q] < 0 || !in_range(fr[q], nf_rows, GS_RESTRICT)) continue;
+        const int ox = q % 3 - 1, oy = (q / 3) % 3 - 1, oz = q / 9 - 1;
+        double w = 1.0;
+        w *= ox == 0 ? 1.0 : 0.5;
+        w *= oy == 0 ? 1.0 : 0.5;
+        if (D == 3) w *= oz == 0 ? 1.0 : 0.5;
+        const uint8_t fx = ffixed[fr[q]];
+#pragma unroll
+        for (int f = 0; f < NF; ++f)
+            if (!((fx >> f) & 1)) acc[f] += w * rf[(size_t)fr[q] * NF + f];
+    }
+#pragma unroll
+    for (int f = 0; f < NF; ++f) bc[(size_t)R * NF + f] = acc[f];
+}
+
+// x_f += P x_c through the parent lists
+template <int D, int NF>
+__global__ void k_mg_prolong_list(int n_rows, int nc, const int *__restrict__ parent,
+                                  const uint8_t *__restrict__ ffixed, const double *__restrict__ xc,
+                                  double *__restrict__ xf, const int *__restrict__ skip) {
+    constexpr int PN = D == 2 ? 4 : 8;
+    if (skip && *skip) return;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    const int *pa = parent + (size_t)r * PN;
+    int R[PN];
+#pragma unroll
+    for (int q = 0; q < PN; ++q) R[q] = pa[q];
+    int cnt = 0;
+#pragma unroll
+    for (int q = 0; q < PN; ++q) cnt += R[q] != -2;
+    const double w = cnt == 1 ? 1.0 : (cnt == 2 ? 0.5 : (cnt == 4 ? 0.25 : 0.125));
+    double acc[NF];
+#pragma unroll
+    for (int f = 0; f < NF; ++f) acc[f] = 0.0;
+#pragma unroll
+    for (int q = 0; q < PN; ++q) {
+        if (R[q] < 0 || !in_range(R[q], nc, GS_PROLONG)) continue;
+#pragma unroll
+        for (int f = 0; f < NF; ++f) acc[f] += w * xc[(size_t)R[q] * NF + f];
+    }
+    const uint8_t fx = ffixed[r];
+#pragma unroll
+    for (int f = 0; f < NF; ++f)
+        if (!((fx >> f) & 1)) xf[(size_t)r * NF + f] += acc[f];
+}
+
 // ---------------------------------------------------------------- coarsest level
 // dense row-major copy of a block-CSR matrix (M zeroed by the caller)
 template <int NF, typename VT>

@@ -96,7 +96,7 @@ __global__ void k_radix_scatter(const int *__restrict__ kin, const int *__restri
     for (int d = threadIdx.x; d < 256; d += blockDim.x) running[d] = offs[d * nblocks + blockIdx.x];
     const int base = blockIdx.x * kSortTile;
     const int end = min(base + kSortTile, n);
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int w = threadIdx.x >> 5;
     for (int chunk = base; chunk < end; chunk += blockDim.x) {
         for (int k = threadIdx.x; k < kSortWarps * 256; k += blockDim.x) (&wcnt[0][0])[k] = 0;
         __syncthreads();
