@@ -115,6 +115,12 @@ class Engine:
         self.precond = PRECONDS[precond]
         self.krylov_rtol = krylov_rtol if krylov_rtol is not None else (1e-12 if precision == "fp64" else 1e-6)
         self.final_krylov_rtol = 1e-6  # solve tolerance of the update taken at ||R|| < tol
+        # inexact-Newton forcing (mixed precision only): each correction is
+        # solved to rtol = clamp(forcing * tol / ||R||, krylov_rtol, forcing_max),
+        # i.e. only as accurately as reaching ||R|| < tol needs; None keeps the
+        # reference's full solves (the FP64 drop-in)
+        self.newton_forcing = 0.1 if precision == "mixed" else None
+        self.forcing_max = 0.1
         self.krylov_max_iter = krylov_max_iter
         if krylov not in ("gmres", "bicgstab"):
             raise ValueError(f"unknown Krylov method {krylov!r}")
@@ -462,6 +468,20 @@ class Engine:
         return v.value
 
     # ------------------------------------------------------------------ Newton
+    def newton_rtol(self, nrm, tol):
+        """Krylov tolerance of the Newton correction at residual norm nrm.
+
+        Without forcing: krylov_rtol (None), or final_krylov_rtol for the last
+        update, taken at ||R|| < tol.  With forcing f (mixed precision): the
+        inexact-Newton bound f * tol / ||R||, clamped to [krylov_rtol,
+        forcing_max]: the next residual is about rtol * ||R|| plus the
+        quadratic and FP32-Jacobian terms, so f = 0.1 leaves it a decade under
+        tol without solving the correction past what the tolerance needs."""
+        if self.newton_forcing is None:
+            return None if nrm >= tol else max(self.krylov_rtol, self.final_krylov_rtol)
+        eta = self.newton_forcing * tol / nrm if nrm > 0 else self.forcing_max
+        return min(self.forcing_max, max(self.krylov_rtol, eta))
+
     def newton(self, mat_struct, current_step, total_steps, n_iter, tol):
         """Newton loop with the reference's stopping rule
         (solvers/quasi_static_solver_2d.py:151-231): R is assembled before the
@@ -494,7 +514,7 @@ class Engine:
             # applies it, then stops); a 1e-6 relative solve moves u by far
             # less than the converged tolerance and spares a Krylov solve that
             # would chase a residual at the FP64 rounding floor
-            kit, relres, rc = self.krylov(None if nrm >= tol else max(self.krylov_rtol, self.final_krylov_rtol))
+            kit, relres, rc = self.krylov(self.newton_rtol(nrm, tol))
             if growth:
                 prev = (self.u_new.clone(), self._delta[:n].clone(), nrm)
                 alpha = 1.0

@@ -22,11 +22,16 @@ def test_batched_blocks_step_like_separate_runs(cuda, precision):
     from geowarp_b200.batch import BatchedBlocks
     fields = _fields(11)
     bb = BatchedBlocks(SIZES, logE=np.concatenate(fields), precision=precision, tol=1e-7)
+    # the mixed engine's inexact-Newton forcing scales each Krylov tolerance by
+    # the whole system's ||R||, so packed and separate runs take other (equally
+    # converged) iterates; the packing itself is checked with full solves
+    bb.solver.engine.newton_forcing = None
     for k in range(3):
         bb.solver.advance_one_step(k, 6)
     d_batch = bb.displacement().cpu().numpy()
     for q, (size, f) in enumerate(zip(SIZES, fields)):
         one = BatchedBlocks([size], logE=f, precision=precision, tol=1e-7)
+        one.solver.engine.newton_forcing = None
         for k in range(3):
             one.solver.advance_one_step(k, 6)
         d_one = one.displacement().cpu().numpy()
