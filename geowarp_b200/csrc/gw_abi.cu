@@ -354,8 +354,6 @@ extern "C" int gw_profile_read(int32_t cls, double *ms_total_host, int64_t *laun
         g_prof_ms[r.cls] += ms;
         g_prof_bytes[r.cls] += r.bytes;
         g_prof_count[r.cls] += 1;
-        cudaEventDestroy(r.a);
-        cudaEventDestroy(r.b);
     }
     g_prof_n = 0;
     *ms_total_host = g_prof_ms[cls];
@@ -365,8 +363,7 @@ extern "C" int gw_profile_read(int32_t cls, double *ms_total_host, int64_t *laun
 }
 
 extern "C" int gw_profile_reset(void) {
-    for (int i = 0; i < g_prof_n; ++i) { cudaEventDestroy(g_prof[i].a); cudaEventDestroy(g_prof[i].b); }
-    g_prof_n = 0;
+    g_prof_n = 0;  // the event pairs stay in the pool
     for (int c = 0; c < PC_COUNT; ++c) { g_prof_ms[c] = 0.0; g_prof_bytes[c] = 0.0; g_prof_count[c] = 0; }
     return GW_OK;
 }

@@ -509,8 +509,10 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
                cudaStream_t s) {
     const MgLevel &v = h.lv[l];
     PtrsA a = make_ptrs(v.A);
-    const int g = zero ? red_grid_elems(v.A.n_rows) : tune_rows_grid(v.A.n_rows);
     const int tb = zero ? kThreads : tune_rows_block();
+    const int g = zero ? red_grid_elems(v.A.n_rows)
+                       : (l == 0 ? resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, v.A.n_rows)
+                                 : resident_rows_grid((const void *)k_mg_jacobi<NF, double>, tb, v.A.n_rows));
     // algorithmic bytes: b, x_out, Minv; with a previous iterate also x_in and the matrix
     const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
     ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
@@ -647,10 +649,14 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
             const double mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
             ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
             if (l == 0)
-                k_mg_presmooth2<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
+                k_mg_presmooth2<NF, VT><<<gw_count_launch(resident_rows_grid(
+                                              (const void *)k_mg_presmooth2<NF, VT>, tune_rows_block(), v.A.n_rows)),
+                                          tune_rows_block(), 0, s>>>(
                     a, v.Minv, v.b, y, mg_omega(), skip);
             else
-                k_mg_presmooth2<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(
+                k_mg_presmooth2<NF, double><<<gw_count_launch(resident_rows_grid(
+                                                  (const void *)k_mg_presmooth2<NF, double>, tune_rows_block(), v.A.n_rows)),
+                                              tune_rows_block(), 0, s>>>(
                     a, v.Minv, v.b, y, mg_omega(), skip);
             double *t = x; x = y; y = t;
             for (int it = 2; it < mg_sweeps(l); ++it) {
@@ -668,8 +674,14 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         const double vs = 8.0 * v.A.n_rows * NF;
         {
         ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4));
-        if (l == 0) k_mg_residual<NF, VT><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
-        else k_mg_residual<NF, double><<<gw_count_launch(tune_rows_grid(v.A.n_rows)), tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
+        if (l == 0)
+            k_mg_residual<NF, VT><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, VT>,
+                                                                       tune_rows_block(), v.A.n_rows)),
+                                    tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
+        else
+            k_mg_residual<NF, double><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, double>,
+                                                                           tune_rows_block(), v.A.n_rows)),
+                                        tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
         }
         ProfScope ps(PC_MG_TRANSFER, s, vs + 8.0 * c.A.n_rows * NF);
         if (D == 2)
@@ -749,7 +761,8 @@ int capture_stream(cudaStream_t *out) {
 template <int NF, typename VT>
 void mg_arnoldi_step(const MgHier &h, const PtrsA &a, const GmresVecs &G, double *Z, int gr, int gv, size_t n,
                      const int *skip, cudaStream_t s) {
-    k_gm_spmv_keep<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, Z);
+    k_gm_spmv_keep<NF, VT><<<gw_count_launch(resident_rows_grid((const void *)k_gm_spmv_keep<NF, VT>, kThreads, a.n_rows)),
+                             kThreads, 0, s>>>(a, G, Z);
     k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0);
     k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0);
     k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1);
@@ -822,7 +835,17 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
     const int nr = A->n_rows;
     if (nr == 0) { *iters = 0; *relres = 0.0; return GW_OK; }
     const int64_t n = (int64_t)nr * NF;
-    (void)tail_cluster_size<NF>(grid->dim);  // device query before any stream capture
+    (void)tail_cluster_size<NF>(grid->dim);  // device queries before any stream capture
+    {
+        const int tb = tune_rows_block();
+        (void)resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_jacobi<NF, double>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_presmooth2<NF, VT>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_presmooth2<NF, double>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_residual<NF, VT>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_residual<NF, double>, tb, 1);
+        (void)resident_rows_grid((const void *)k_gm_spmv_keep<NF, VT>, kThreads, 1);
+    }
     Bump bp{(char *)ws, 0};
     MgHier h;
     FlexVecs fv;
@@ -867,6 +890,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
     const double eta2 = ::pow(10.0, -0.1 * g_tune[GW_TUNE_GS_CANCEL]);
     GW_CUDA(cudaMemcpyAsync(&G.sc->gs_eta2, &eta2, sizeof(double), cudaMemcpyHostToDevice, s));
     const int gr = red_grid_rows(nr), gv = red_grid_elems(n);
+    const int gk = resident_rows_grid((const void *)k_gm_spmv_keep<NF, VT>, kThreads, nr);
     const int *skip = &G.sc->cycle_done;
     GScalars hs;
     memset(&hs, 0, head);
@@ -905,7 +929,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
                     continue;
                 }
                 const double vb = 8.0 * n * (kk + 2);
-                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv_keep<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, fv.Z); }
+                { ProfScope ps(PC_SPMV, s, spmv_bytes); k_gm_spmv_keep<NF, VT><<<gw_count_launch(gk), kThreads, 0, s>>>(a, G, fv.Z); }
                 { ProfScope ps(PC_DOTS, s, vb + 8.0 * n); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
                 { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
                 const int re = prof_reorth(G.sc, s);

@@ -3,6 +3,7 @@
 // scans and the index-guard check.  State is held in C++17 inline variables,
 // so every translation unit sees one copy; helpers are static inline.
 #pragma once
+#include <mutex>
 #include <stddef.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -49,15 +50,36 @@ inline const char *kProfNames[PC_COUNT] = {"k_assemble", "k_gm_spmv", "k_gm_dots
                                     "k_adjoint_g2p", "k_adjoint_residual", "k_mg_jacobi (finest level)",
                                     "k_mg_residual", "k_mg_restrict/prolong", "mg_setup",
                                     "k_mg_jacobi (coarse levels)", "k_mg_tail (fused coarse levels)"};
-struct ProfRec { int cls; cudaEvent_t a, b; double bytes; };
+// Event pairs are kept in a pool (created once, reused by later records).
+struct ProfRec { int cls; cudaEvent_t a, b; double bytes; bool made; };
 inline bool g_prof_on = false;
 inline ProfRec *g_prof = nullptr;
 inline int g_prof_n = 0, g_prof_cap = 0;
 inline double g_prof_ms[PC_COUNT], g_prof_bytes[PC_COUNT];
 inline long g_prof_count[PC_COUNT];
 
+namespace {
+// A bounded pause of the stream (%globaltimer, at most ns nanoseconds and a
+// fixed number of polls): the host queues the next timed launches meanwhile.
+__global__ void k_prof_delay(long long ns) {
+    long long t0, t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
+    for (int i = 0; i < 1000000; ++i) {
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        if (t - t0 >= ns) break;
+        __nanosleep(500);
+    }
+}
+}  // namespace
+
+// Brackets one launch (or a short sequence) with events on its stream.  The
+// interval [a, b] must not contain host time: when the previous timed launch
+// has already finished, the GPU is idle and would start this launch as soon as
+// the host submits it, so the submission gap would be timed too.  Then a
+// 200-microsecond pause goes in first, and the host queues ahead of the GPU
+// again before the interval opens on the device.
 struct ProfScope {
-    ProfRec *r = nullptr;
+    int idx = -1;
     cudaStream_t s;
     ProfScope(int cls, cudaStream_t st, double bytes) : s(st) {
         if (!g_prof_on) return;
@@ -65,18 +87,24 @@ struct ProfScope {
             int nc = g_prof_cap ? 2 * g_prof_cap : 4096;
             ProfRec *nr = (ProfRec *)realloc(g_prof, sizeof(ProfRec) * nc);
             if (!nr) return;
+            for (int i = g_prof_cap; i < nc; ++i) nr[i].made = false;
             g_prof = nr;
             g_prof_cap = nc;
         }
-        r = &g_prof[g_prof_n++];
-        r->cls = cls;
-        r->bytes = bytes;
-        cudaEventCreate(&r->a);
-        cudaEventCreate(&r->b);
-        cudaEventRecord(r->a, s);
+        idx = g_prof_n++;
+        ProfRec &r = g_prof[idx];
+        r.cls = cls;
+        r.bytes = bytes;
+        if (!r.made) {
+            cudaEventCreate(&r.a);
+            cudaEventCreate(&r.b);
+            r.made = true;
+        }
+        if (idx == 0 || cudaEventQuery(g_prof[idx - 1].b) == cudaSuccess) k_prof_delay<<<1, 1, 0, s>>>(200000);
+        cudaEventRecord(r.a, s);
     }
     ~ProfScope() {
-        if (r) cudaEventRecord(r->b, s);
+        if (idx >= 0) cudaEventRecord(g_prof[idx].b, s);
     }
 };
 // every kernel launch of the library passes its grid size through here, so the
@@ -110,6 +138,37 @@ static inline int red_grid_rows(int n_rows) {
     return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b);
 }
 static inline int red_grid_elems(int64_t n) { int b = nblk(n, kThreads); return b < 1 ? 1 : (b > kRedBlocks ? kRedBlocks : b); }
+
+// Grid of a grid-stride block-row kernel that has no cross-block reduction
+// (each row's result is independent of the grid): the CTAs of `block` threads
+// the device keeps resident at once, so the rows run in one wave with no
+// partly filled last wave, and at most the CTAs the rows need.  The resident
+// count comes from the occupancy calculator once per kernel, block size and
+// device.
+static inline int resident_rows_grid(const void *fn, int block, int n_rows) {
+    struct Ent { const void *fn; int block, dev, nb; };
+    static Ent cache[256];
+    static int n = 0;
+    static std::mutex mu;
+    int dev = 0;
+    (void)cudaGetDevice(&dev);
+    int nb = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (int i = 0; i < n; ++i)
+            if (cache[i].fn == fn && cache[i].block == block && cache[i].dev == dev) { nb = cache[i].nb; break; }
+        if (!nb) {
+            int per = 0, sms = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, block, 0) != cudaSuccess || per < 1) per = 1;
+            if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) sms = 1;
+            (void)cudaGetLastError();
+            nb = per * sms;
+            if (n < 256) cache[n++] = {fn, block, dev, nb};
+        }
+    }
+    const int want = nblk(n_rows, (int64_t)(block / 32) * kRowsPerWarp);
+    return want < 1 ? 1 : (want < nb ? want : nb);
+}
 
 static inline LaunchConst make_lc(const gw_grid_t *g, const gw_material_t *m, const gw_step_t *st) {
     LaunchConst c;
