@@ -52,7 +52,7 @@ extern "C" int gw_adjoint_g2p(const gw_grid_t *grid, const gw_material_t *mat, c
     const PtrsP pp = make_ptrs(*pt);
     const PtrsA pa = make_ptrs(*A);
     const AdjState si = make_adj(*seed_in), qo = make_adj(*q_out);
-    switch (mat->model) {  // one instantiation per material: see solid2d_dual
+    switch (mat->model) {  // one instantiation per material: see solid2d_vjp
         case GW_MODEL_HENCKY: k_adjoint_g2p<GW_MODEL_HENCKY><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
         case GW_MODEL_J2: k_adjoint_g2p<GW_MODEL_J2><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
         case GW_MODEL_DP: k_adjoint_g2p<GW_MODEL_DP><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, si, qo, ubar_rows); break;
@@ -81,7 +81,7 @@ extern "C" int gw_adjoint_residual(const gw_grid_t *grid, const gw_material_t *m
     const PtrsA pa = make_ptrs(*A);
     const AdjState qo = make_adj(*q_out);
     cudaStream_t s = S(stream);
-    switch (mat->model) {  // one instantiation per material: see solid2d_dual
+    switch (mat->model) {  // one instantiation per material: see solid2d_vjp
         case GW_MODEL_HENCKY: k_adjoint_residual<GW_MODEL_HENCKY><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
         case GW_MODEL_J2: k_adjoint_residual<GW_MODEL_J2><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;
         case GW_MODEL_DP: k_adjoint_residual<GW_MODEL_DP><<<grd, blk, 0, s>>>(c, pp, u_new, u_old, free_mask, pa, lambda_rows, qo); break;

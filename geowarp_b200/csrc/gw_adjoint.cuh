@@ -12,14 +12,11 @@
 // residual rows weighted by lambda -- with respect to 19 particle inputs:
 //   inputs 0-1 x, 2-3 lp, 4-8 F_old (00,01,10,11,22), 9-12 b_old (00,01=10,11,22),
 //   13 E, 14-17 H (00,01,10,11), 18 ubar_y (penalty footing).
-// They come from forward-mode dual passes through the same formulas as the
-// forward kernels, chunked: each pass carries kAdjChunk dual lanes (a window
-// of the inputs) and contracts every output with its weight as soon as it is
-// formed, so no per-row Jacobian is kept.  The 19 inputs take seven passes
-// (the residual adjoint, which needs inputs 0-13 only, takes five).  The
-// principal-space constitutive update (eigen-solve and return map) runs once
-// per particle, before the passes, as a 5-lane Jacobian with respect to the
-// trial b and E (constitutive_jac); the passes apply it by the chain rule.
+// They come from one reverse-mode sweep per particle (solid2d_vjp): a forward
+// pass over values, then the chain rule applied backwards through the same
+// formulas as the forward kernels.  The principal-space constitutive update
+// (eigen-solve and return map) enters through its Jacobian with respect to
+// the trial b and E, evaluated once per particle (constitutive_jac).
 #pragma once
 #include "gw_step_kernels.cuh"
 
@@ -27,21 +24,8 @@ namespace gw {
 namespace {  // internal linkage: each translation unit compiles the kernels it launches
 
 constexpr int kAdjInputs = 19;
-constexpr int kAdjChunk = 3;
-constexpr int kAdjLanes = kAdjChunk;  // dual lanes per pass
-typedef Dual<kAdjChunk, double> AD;
+typedef Dual<2, double> AD;  // partials of the 1D shape functions in x and lp
 constexpr int LX = 0, LLP = 2, LF = 4, LB = 9, LE = 13, LH = 14, LU = 18;
-
-// adds val to the lane of input `input` when it falls in this pass's window
-GW_HD void set_lane(AD &v, int input, int off, double val = 1.0) {
-    const int l = input - off;
-    if (l >= 0 && l < kAdjChunk) v.d[l] += val;
-}
-GW_HD AD seed(double v, int input, int off) {
-    AD r(v);
-    set_lane(r, input, off);
-    return r;
-}
 
 // cpGIMP axis with dual position and half-width; the cell indices come from
 // the values (piecewise-constant), the weights carry the lanes.
@@ -149,9 +133,9 @@ GW_HD void principal_tangent_E(const LaunchConst &c, int model, double Ev, const
 // is eigen-decomposed once, each direction is rotated into its frame, the
 // principal derivatives come from the return map's algorithmic tangent, and
 // the isotropic tensor functions are assembled back with their coalescence
-// limits.  Every chunked pass then takes tau's and b_new's lanes from this
-// record by the chain rule, so the eigen-solve and the return map run once
-// per particle instead of once per pass.
+// limits.  The reverse sweep takes tau's and b_new's adjoints back to the
+// trial b and E through this record, so the eigen-solve and the return map
+// run once per particle.
 constexpr int kCJ = 5;
 struct ConstJac {
     double tv[4], Jt[4][kCJ];  // tau
@@ -224,193 +208,335 @@ GW_HD void constitutive_jac(const LaunchConst &c, int model, const double B[3][3
     }
 }
 
-// out (tau or b_new) with this pass's lanes: value from the Jacobian record,
-// lanes = J (d b_trial components, d E).
-GW_HD void apply_cjac(const double v[4], const double J[4][kCJ], const AD btr[3][3], const AD &E, AD out[3][3]) {
-    AD q[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        q[k] = AD(v[k]);
-#pragma unroll
-        for (int l = 0; l < kAdjLanes; ++l)
-            q[k].d[l] = J[k][0] * btr[0][0].d[l] + J[k][1] * btr[0][1].d[l] + J[k][2] * btr[1][1].d[l] +
-                        J[k][3] * btr[2][2].d[l] + J[k][4] * E.d[l];
-    }
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) out[i][j] = AD(0.0);
-    out[0][0] = q[0];
-    out[0][1] = q[1];
-    out[1][0] = q[1];
-    out[1][1] = q[2];
-    out[2][2] = q[3];
-}
-
 // Weights of the contracted outputs: lambda per slot and field for the
 // residual rows (zero on fixed DOFs), and / or the seeds of the G2P outputs.
-struct DualWeights {
+struct VjpWeights {
     const double (*r)[2];           // [9][2] or null
     const double *x, *lp, *F, *b;   // G2P seeds ([2], [2], [9], [9]) or null
 };
 
-struct SolidDual {
-    AD s;               // sum(output . weight) with this pass's lanes
+struct ParticleAdj {  // shape data of the particle's 9 slots, for the nodal adjoint
     int nid[9];
     double W[9], G[9][2];
     int lower[2], span[2];
     double xnew_dx[2];  // d lp_new_k / d x_new_k (clip branch: 0, +1 or -1)
 };
 
-// Forward pass of one 2D solid particle in dual arithmetic, lanes for inputs
-// off .. off + kAdjChunk - 1.  du: nodal increments of the 9 slots (u_new -
-// u_old), values only.  MODEL is the material (GW_MODEL_*) fixed at compile
-// time, so an instantiation carries only its own constitutive code; MODEL < 0
-// reads it from c at run time.
+// Reverse-mode VJP of one 2D solid particle: q[i] = ds / d input_i for the 19
+// inputs, with s = sum(output . weight).  One forward pass
+// keeps the values (and the 1D shape functions' partials in x and lp, from a
+// 2-lane dual evaluation per axis); the sweep then applies the chain rule
+// backwards through the same formulas: G2P outputs, residual rows, penalty,
+// stress (principal-space models through the constitutive Jacobian cj;
+// neo-Hookean and linear in closed form), F_new = f F_old, b_trial = f b_old
+// f^T, f^-1, f = I + H, the gathered H / ubar / dx, and the shape functions.
+// Nothing is recomputed per input, so the particle's state stays in registers.
 template <int MODEL>
-GW_HD void solid2d_dual(const LaunchConst &c, const double *xv, const double *lpv, const double *Fo_v,
-                        const double *bo_v, double Ev, const double fext[2], const double du[9][2], int off,
-                        const DualWeights &wt, ConstJac &cj, SolidDual &o) {
+__device__ __forceinline__ void solid2d_vjp(const LaunchConst &c, const double *xv, const double *lpv,
+                                            const double *Fo_v, const double *bo_v, double Ev, const double fext[2],
+                                            const double du[9][2], const VjpWeights &wt, const ConstJac &cj,
+                                            double q[kAdjInputs], ParticleAdj &o) {
     const gw_grid_t &g = c.g;
     const bool want_g2p = wt.x != nullptr;
-    o.s = AD(0.0);
-    AD x[2] = {seed(xv[0], LX, off), seed(xv[1], LX + 1, off)};
-    AD lp[2] = {seed(lpv[0], LLP, off), seed(lpv[1], LLP + 1, off)};
-    AD Fo[3][3], bo[3][3];
-    for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) { Fo[i][j] = AD(Fo_v[i * 3 + j]); bo[i][j] = AD(bo_v[i * 3 + j]); }
-    set_lane(Fo[0][0], LF, off); set_lane(Fo[0][1], LF + 1, off); set_lane(Fo[1][0], LF + 2, off);
-    set_lane(Fo[1][1], LF + 3, off); set_lane(Fo[2][2], LF + 4, off);
-    set_lane(bo[0][0], LB, off); set_lane(bo[0][1], LB + 1, off); set_lane(bo[1][0], LB + 1, off);
-    set_lane(bo[1][1], LB + 2, off); set_lane(bo[2][2], LB + 3, off);
-    AD E = seed(Ev, LE, off);
+    const int model = MODEL >= 0 ? MODEL : c.mc.model;
+    const bool spectral = model == GW_MODEL_HENCKY || model == GW_MODEL_J2 || model == GW_MODEL_DP;
     const double nu = c.nu;
-    AD lam = E * (nu / ((1.0 + nu) * (1.0 - 2.0 * nu)));
-    AD mu = E * (1.0 / (2.0 * (1.0 + nu)));
+    const double cl = nu / ((1.0 + nu) * (1.0 - 2.0 * nu)), cm = 1.0 / (2.0 * (1.0 + nu));
+    const double lam = Ev * cl, mu = Ev * cm;
 
-    AD w[2][3], gw[2][3];
-    for (int k = 0; k < 2; ++k) gimp_axis_dual(x[k], lp[k], g.h[k], g.inv_h[k], o.lower[k], o.span[k], w[k], gw[k]);
-    AD W[9], G[9][2];
+    // ---------------- forward values
+    double w[2][3], gw[2][3], dw[2][3][2], dgw[2][3][2];  // [axis][node], partials [d/dx, d/dlp]
+    for (int k = 0; k < 2; ++k) {
+        AD xd(xv[k]), ld(lpv[k]);
+        xd.d[0] = 1.0;
+        ld.d[1] = 1.0;
+        AD wd[3], gd[3];
+        gimp_axis_dual(xd, ld, g.h[k], g.inv_h[k], o.lower[k], o.span[k], wd, gd);
+        for (int i = 0; i < 3; ++i) {
+            w[k][i] = wd[i].v;
+            gw[k][i] = gd[i].v;
+            dw[k][i][0] = wd[i].d[0];
+            dw[k][i][1] = wd[i].d[1];
+            dgw[k][i][0] = gd[i].d[0];
+            dgw[k][i][1] = gd[i].d[1];
+        }
+    }
     for (int a = 0; a < 9; ++a) {
         const int i = a % 3, j = a / 3;
-        W[a] = w[0][i] * w[1][j];
-        G[a][0] = gw[0][i] * w[1][j];
-        G[a][1] = w[0][i] * gw[1][j];
-        o.W[a] = W[a].v;
-        o.G[a][0] = G[a][0].v;
-        o.G[a][1] = G[a][1].v;
+        o.W[a] = w[0][i] * w[1][j];
+        o.G[a][0] = gw[0][i] * w[1][j];
+        o.G[a][1] = w[0][i] * gw[1][j];
         const int cx = o.lower[0] + i, cy = o.lower[1] + j;
         o.nid[a] = (cx >= 0 && cx <= g.n_grid[0] && cy >= 0 && cy <= g.n_grid[1]) ? cx + cy * (g.n_grid[0] + 1) : -1;
     }
-    AD H[2][2], ubar(0.0);
-    for (int k = 0; k < 2; ++k)
-        for (int l = 0; l < 2; ++l) H[k][l] = AD(0.0);
-    AD dx_p[2] = {AD(0.0), AD(0.0)};
+    double H[2][2] = {{0.0, 0.0}, {0.0, 0.0}}, ubar = 0.0, dxp[2] = {0.0, 0.0};
     for (int a = 0; a < 9; ++a) {
         if (o.nid[a] < 0) continue;
         for (int k = 0; k < 2; ++k)
-            for (int l = 0; l < 2; ++l) H[k][l] += G[a][k] * du[a][l];
-        ubar += W[a] * du[a][1];
-        dx_p[0] += W[a] * du[a][0];
-        dx_p[1] += W[a] * du[a][1];
+            for (int l = 0; l < 2; ++l) H[k][l] += o.G[a][k] * du[a][l];
+        ubar += o.W[a] * du[a][1];
+        dxp[0] += o.W[a] * du[a][0];
+        dxp[1] += o.W[a] * du[a][1];
     }
-    set_lane(H[0][0], LH, off); set_lane(H[0][1], LH + 1, off); set_lane(H[1][0], LH + 2, off);
-    set_lane(H[1][1], LH + 3, off);
-    set_lane(ubar, LU, off);
-
-    // kinematics
-    AD Finc[3][3];
+    double Fi[3][3] = {{1.0 + H[0][0], H[0][1], 0.0}, {H[1][0], 1.0 + H[1][1], 0.0}, {0.0, 0.0, 1.0}};
+    const double det2 = Fi[0][0] * Fi[1][1] - Fi[0][1] * Fi[1][0];
+    const double Finv[2][2] = {{Fi[1][1] / det2, -Fi[0][1] / det2}, {-Fi[1][0] / det2, Fi[0][0] / det2}};
+    double Fo[3][3], bo[3][3], Fn[3][3];
     for (int i = 0; i < 3; ++i)
-        for (int j = 0; j < 3; ++j) Finc[i][j] = AD(i == j ? 1.0 : 0.0);
-    for (int i = 0; i < 2; ++i)
-        for (int j = 0; j < 2; ++j) Finc[i][j] += H[i][j];
-    AD det2 = Finc[0][0] * Finc[1][1] - Finc[0][1] * Finc[1][0];
-    AD Finv[2][2] = {{Finc[1][1] / det2, -Finc[0][1] / det2}, {-Finc[1][0] / det2, Finc[0][0] / det2}};
-    AD F_new[3][3];
-    matmul3(Finc, Fo, F_new);
-    AD J = det3(F_new);
-    AD btr[3][3];
-    congruence3(Finc, bo, btr);
-    if (want_g2p)  // F_new is a G2P output
+        for (int j = 0; j < 3; ++j) { Fo[i][j] = Fo_v[i * 3 + j]; bo[i][j] = bo_v[i * 3 + j]; }
+    matmul3(Fi, Fo, Fn);
+    const double J = det3(Fn);
+    double tau[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double lnJ = 0.0, eps[3][3], tr = 0.0, sg[3][3];
+    if (spectral) {
+        tau[0][0] = cj.tv[0];
+        tau[0][1] = tau[1][0] = cj.tv[1];
+        tau[1][1] = cj.tv[2];
+        tau[2][2] = cj.tv[3];
+    } else if (model == GW_MODEL_NEOHOOKEAN) {
+        lnJ = ::log(J);
         for (int i = 0; i < 3; ++i)
-            for (int j = 0; j < 3; ++j) o.s += F_new[i][j] * wt.F[i * 3 + j];
-
-    // stress (Kirchhoff) and b_new
-    AD tau[3][3];
-    const int model = MODEL >= 0 ? MODEL : c.mc.model;
-    if (model == GW_MODEL_HENCKY || model == GW_MODEL_J2 || model == GW_MODEL_DP) {
-        apply_cjac(cj.tv, cj.Jt, btr, E, tau);
-        if (want_g2p) {  // b_new is a G2P output
-            AD bn[3][3];
-            apply_cjac(cj.bv, cj.Jb, btr, E, bn);
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) o.s += bn[i][j] * wt.b[i * 3 + j];
-        }
+            for (int j = 0; j < 3; ++j) {
+                const double ff = Fn[i][0] * Fn[j][0] + Fn[i][1] * Fn[j][1] + Fn[i][2] * Fn[j][2];
+                tau[i][j] = mu * (ff - (i == j ? 1.0 : 0.0));
+                if (i == j) tau[i][j] += lam * lnJ;
+            }
     } else {
-        if (want_g2p)
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) o.s += btr[i][j] * wt.b[i * 3 + j];
-        if (model == GW_MODEL_NEOHOOKEAN) {  // J sigma = mu (F F^T - I) + lam ln J I
-            AD lnJ = glog(J);
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    AD ff = F_new[i][0] * F_new[j][0] + F_new[i][1] * F_new[j][1] + F_new[i][2] * F_new[j][2];
-                    tau[i][j] = mu * (ff - (i == j ? 1.0 : 0.0));
-                    if (i == j) tau[i][j] += lam * lnJ;
-                }
-        } else {  // linear: sigma = lam tr(eps) I + 2 mu eps, tau = J sigma
-            AD eps[3][3];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) eps[i][j] = (F_new[i][j] + F_new[j][i]) * 0.5 - (i == j ? 1.0 : 0.0);
-            AD tr = eps[0][0] + eps[1][1] + eps[2][2];
-            for (int i = 0; i < 3; ++i)
-                for (int j = 0; j < 3; ++j) {
-                    AD sg = mu * 2.0 * eps[i][j];
-                    if (i == j) sg += lam * tr;
-                    tau[i][j] = J * sg;
-                }
-        }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) eps[i][j] = (Fn[i][j] + Fn[j][i]) * 0.5 - (i == j ? 1.0 : 0.0);
+        tr = eps[0][0] + eps[1][1] + eps[2][2];
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                sg[i][j] = mu * 2.0 * eps[i][j];
+                if (i == j) sg[i][j] += lam * tr;
+                tau[i][j] = J * sg[i][j];
+            }
     }
-
-    // residual rows (mpm/mpm_utils.py:575-596): r_a = -(Finv G_a)^T tau2 V0 + W_a rho0 V0 g + W_a f_ext + pen W_a
     const double V0 = c.st.p_vol;
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
     const double gv = -c.st.gravity_mag * (c.st.gravity_full ? 1.0 : ramp);
-    AD pen(0.0);
     bool pen_on = false;
+    double pen = 0.0, height = 0.0, pa = 0.0, sgn = 1.0;
     if (c.st.has_footing) {
-        const double height = c.st.footing_initial_height + (c.st.current_step + 1.0) * c.st.footing_incr_disp;
+        height = c.st.footing_initial_height + (c.st.current_step + 1.0) * c.st.footing_incr_disp;
         if (xv[1] >= height && xv[0] > c.st.footing_min[0] && xv[0] < c.st.footing_max[0]) {
-            const double area = c.g.h[0] / c.st.PPD;
-            AD kp = E * (c.st.penalty_factor * area);
-            pen = -((height - (x[1] + ubar)) * kp);
-            if (c.st.footing_stable) pen = -pen;
+            pa = c.st.penalty_factor * (c.g.h[0] / c.st.PPD);
+            sgn = c.st.footing_stable ? -1.0 : 1.0;
+            pen = sgn * (xv[1] + ubar - height) * (Ev * pa);
             pen_on = true;
         }
     }
-    if (wt.r)
+
+    // ---------------- reverse sweep
+    double xb[2] = {0.0, 0.0}, lpb[2] = {0.0, 0.0}, Eb = 0.0, ubarb = 0.0, dxb[2] = {0.0, 0.0}, penb = 0.0;
+    double Fnb[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double Btb[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double taub[3][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    double Wb[9], Gb[9][2], Finvb[2][2] = {{0.0, 0.0}, {0.0, 0.0}};
+    for (int a = 0; a < 9; ++a) { Wb[a] = 0.0; Gb[a][0] = Gb[a][1] = 0.0; }
+    if (want_g2p) {  // x_new = x + dx ; lp_new from F_new's columns (clipped) ; F_new
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) Fnb[i][j] += wt.F[i * 3 + j];
+        for (int k = 0; k < 2; ++k) {
+            const double xn = xv[k] + dxp[k];
+            const double U = ::sqrt(Fn[0][k] * Fn[0][k] + Fn[1][k] * Fn[1][k] + Fn[2][k] * Fn[2][k]);
+            double v = U * c.st.lp0;
+            int br = 0;
+            if (xn - v < c.g.domain_min[k]) { v = xn - (c.g.domain_min[k] + 1e-6); br = 1; }
+            if (xn + v > c.g.domain_max[k]) { v = (c.g.domain_max[k] - 1e-6) - xn; br = 2; }
+            double xnb = wt.x[k];
+            const double vb = wt.lp[k];
+            if (br == 0) {
+                const double Ub = vb * c.st.lp0;
+                for (int i = 0; i < 3; ++i) Fnb[i][k] += Ub * Fn[i][k] / U;
+            } else {
+                xnb += br == 1 ? vb : -vb;
+            }
+            o.xnew_dx[k] = br == 0 ? 0.0 : (br == 1 ? 1.0 : -1.0);
+            xb[k] += xnb;
+            dxb[k] += xnb;
+        }
+    }
+    if (wt.r)  // r_a = -(f^-T G_a) . tau V0 + W_a (rho V0 g + pen + f_ext)
         for (int a = 0; a < 9; ++a) {
             if (wt.r[a][0] == 0.0 && wt.r[a][1] == 0.0) continue;
-            AD wg[2];
-            for (int i = 0; i < 2; ++i) wg[i] = Finv[i][0] * G[a][0] + Finv[i][1] * G[a][1];
+            double wg[2], wgb[2] = {0.0, 0.0};
+            for (int i = 0; i < 2; ++i) wg[i] = Finv[i][0] * o.G[a][0] + Finv[i][1] * o.G[a][1];
             for (int j = 0; j < 2; ++j) {
-                AD v = -(wg[0] * tau[0][j] + wg[1] * tau[1][j]) * V0;
-                if (j == 1) v += W[a] * (c.st.p_rho * V0 * gv);
-                if (j == 1 && pen_on) v += pen * W[a];
-                v += W[a] * fext[j];
-                o.s += v * wt.r[a][j];
+                const double lr = wt.r[a][j];
+                wgb[0] -= tau[0][j] * V0 * lr;
+                wgb[1] -= tau[1][j] * V0 * lr;
+                taub[0][j] -= wg[0] * V0 * lr;
+                taub[1][j] -= wg[1] * V0 * lr;
+                double wc = fext[j];
+                if (j == 1) wc += c.st.p_rho * V0 * gv;
+                if (j == 1 && pen_on) {
+                    wc += pen;
+                    penb += o.W[a] * lr;
+                }
+                Wb[a] += wc * lr;
+            }
+            for (int m = 0; m < 2; ++m) {
+                Gb[a][m] += wgb[0] * Finv[0][m] + wgb[1] * Finv[1][m];
+                for (int i = 0; i < 2; ++i) Finvb[i][m] += wgb[i] * o.G[a][m];
             }
         }
-    if (!want_g2p) return;
-    // G2P outputs: x_new = x + sum W du ; lp_new from F_new columns, clipped
-    for (int k = 0; k < 2; ++k) {
-        const AD xn = x[k] + dx_p[k];
-        AD U = gsqrt(F_new[0][k] * F_new[0][k] + F_new[1][k] * F_new[1][k] + F_new[2][k] * F_new[2][k]);
-        AD v = U * c.st.lp0;
-        double dxd = 0.0;
-        if (xn.v - v.v < c.g.domain_min[k]) { v = xn - (c.g.domain_min[k] + 1e-6); dxd = 1.0; }
-        if (xn.v + v.v > c.g.domain_max[k]) { v = (c.g.domain_max[k] - 1e-6) - xn; dxd = -1.0; }
-        o.s += xn * wt.x[k] + v * wt.lp[k];
-        o.xnew_dx[k] = dxd;
+    if (pen_on) {  // pen = sgn (x1 + ubar - height) E pa
+        xb[1] += sgn * Ev * pa * penb;
+        ubarb += sgn * Ev * pa * penb;
+        Eb += sgn * (xv[1] + ubar - height) * pa * penb;
     }
+    double Jb = 0.0;
+    if (spectral) {  // tau, b_new from the constitutive Jacobian (components 00, 01 = 10, 11, 22)
+        const double qb[4] = {taub[0][0], taub[0][1] + taub[1][0], taub[1][1], taub[2][2]};
+        double pb[4] = {0.0, 0.0, 0.0, 0.0};
+        if (want_g2p) {
+            pb[0] = wt.b[0];
+            pb[1] = wt.b[1] + wt.b[3];
+            pb[2] = wt.b[4];
+            pb[3] = wt.b[8];
+        }
+        double bc[5];
+        for (int m = 0; m < kCJ; ++m) {
+            double v = 0.0;
+            for (int k = 0; k < 4; ++k) v += qb[k] * cj.Jt[k][m];
+            if (want_g2p)
+                for (int k = 0; k < 4; ++k) v += pb[k] * cj.Jb[k][m];
+            bc[m] = v;
+        }
+        Btb[0][0] += bc[0];
+        Btb[0][1] += 0.5 * bc[1];
+        Btb[1][0] += 0.5 * bc[1];
+        Btb[1][1] += bc[2];
+        Btb[2][2] += bc[3];
+        Eb += bc[4];
+    } else {
+        if (want_g2p)  // b_new = b_trial
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) Btb[i][j] += wt.b[i * 3 + j];
+        double mub = 0.0, lamb = 0.0;
+        if (model == GW_MODEL_NEOHOOKEAN) {  // tau = mu (F F^T - I) + lam ln J I
+            for (int i = 0; i < 3; ++i)
+                for (int k = 0; k < 3; ++k) {
+                    double v = 0.0;
+                    for (int j = 0; j < 3; ++j) v += (taub[i][j] + taub[j][i]) * Fn[j][k];
+                    Fnb[i][k] += mu * v;
+                }
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    const double ff = Fn[i][0] * Fn[j][0] + Fn[i][1] * Fn[j][1] + Fn[i][2] * Fn[j][2];
+                    mub += taub[i][j] * (ff - (i == j ? 1.0 : 0.0));
+                }
+            const double trb = taub[0][0] + taub[1][1] + taub[2][2];
+            lamb += lnJ * trb;
+            Jb += lam * trb / J;
+        } else {  // linear: tau = J (2 mu eps + lam tr(eps) I), eps = sym(F) - I
+            double sgb[3][3], trs = 0.0;
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    sgb[i][j] = J * taub[i][j];
+                    Jb += taub[i][j] * sg[i][j];
+                }
+            for (int i = 0; i < 3; ++i) trs += sgb[i][i];
+            for (int i = 0; i < 3; ++i)
+                for (int j = 0; j < 3; ++j) {
+                    mub += 2.0 * sgb[i][j] * eps[i][j];
+                    const double eb = 2.0 * mu * sgb[i][j] + (i == j ? lam * trs : 0.0);
+                    Fnb[i][j] += 0.5 * eb;
+                    Fnb[j][i] += 0.5 * eb;
+                }
+            lamb += tr * trs;
+        }
+        Eb += mub * cm + lamb * cl;
+    }
+    if (Jb != 0.0) {  // d det(F) / dF = cofactor matrix
+        Fnb[0][0] += Jb * (Fn[1][1] * Fn[2][2] - Fn[1][2] * Fn[2][1]);
+        Fnb[0][1] += Jb * (Fn[1][2] * Fn[2][0] - Fn[1][0] * Fn[2][2]);
+        Fnb[0][2] += Jb * (Fn[1][0] * Fn[2][1] - Fn[1][1] * Fn[2][0]);
+        Fnb[1][0] += Jb * (Fn[0][2] * Fn[2][1] - Fn[0][1] * Fn[2][2]);
+        Fnb[1][1] += Jb * (Fn[0][0] * Fn[2][2] - Fn[0][2] * Fn[2][0]);
+        Fnb[1][2] += Jb * (Fn[0][1] * Fn[2][0] - Fn[0][0] * Fn[2][1]);
+        Fnb[2][0] += Jb * (Fn[0][1] * Fn[1][2] - Fn[0][2] * Fn[1][1]);
+        Fnb[2][1] += Jb * (Fn[0][2] * Fn[1][0] - Fn[0][0] * Fn[1][2]);
+        Fnb[2][2] += Jb * (Fn[0][0] * Fn[1][1] - Fn[0][1] * Fn[1][0]);
+    }
+    // F_new = f F_old ; b_trial = f b_old f^T (b_old symmetric) ; f^-1
+    double Fib[3][3], Fob[3][3], bob[3][3];
+    {
+        double S[3][3], T[3][3];  // S = Btb + Btb^T ; T = f b_old
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) S[i][j] = Btb[i][j] + Btb[j][i];
+        matmul3(Fi, bo, T);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int k = 0; k < 3; ++k) v += Fnb[i][k] * Fo[j][k] + S[i][k] * T[k][j];
+                Fib[i][j] = v;
+                double u = 0.0;
+                for (int k = 0; k < 3; ++k) u += Fi[k][i] * Fnb[k][j];
+                Fob[i][j] = u;
+            }
+        double U2[3][3];  // f^T Btb f
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int k = 0; k < 3; ++k) v += Btb[i][k] * Fi[k][j];
+                U2[i][j] = v;
+            }
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j) {
+                double v = 0.0;
+                for (int k = 0; k < 3; ++k) v += Fi[k][i] * U2[k][j];
+                bob[i][j] = v;
+            }
+    }
+    for (int i = 0; i < 2; ++i)  // d f^-1 = -f^-1 df f^-1
+        for (int j = 0; j < 2; ++j) {
+            double v = 0.0;
+            for (int k = 0; k < 2; ++k)
+                for (int m = 0; m < 2; ++m) v += Finv[k][i] * Finvb[k][m] * Finv[j][m];
+            Fib[i][j] -= v;
+        }
+    // f = I + H ; H, ubar, dx gathered from the slots
+    const double Hb[2][2] = {{Fib[0][0], Fib[0][1]}, {Fib[1][0], Fib[1][1]}};
+    for (int a = 0; a < 9; ++a) {
+        if (o.nid[a] < 0) continue;
+        for (int k = 0; k < 2; ++k) Gb[a][k] += Hb[k][0] * du[a][0] + Hb[k][1] * du[a][1];
+        Wb[a] += ubarb * du[a][1] + dxb[0] * du[a][0] + dxb[1] * du[a][1];
+    }
+    // W = w0 w1, G = (gw0 w1, w0 gw1) ; 1D weights -> x, lp
+    double wb[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}}, gwb[2][3] = {{0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    for (int a = 0; a < 9; ++a) {
+        const int i = a % 3, j = a / 3;
+        wb[0][i] += Wb[a] * w[1][j] + Gb[a][1] * gw[1][j];
+        wb[1][j] += Wb[a] * w[0][i] + Gb[a][0] * gw[0][i];
+        gwb[0][i] += Gb[a][0] * w[1][j];
+        gwb[1][j] += Gb[a][1] * w[0][i];
+    }
+    for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < 3; ++i) {
+            xb[k] += wb[k][i] * dw[k][i][0] + gwb[k][i] * dgw[k][i][0];
+            lpb[k] += wb[k][i] * dw[k][i][1] + gwb[k][i] * dgw[k][i][1];
+        }
+    q[LX] = xb[0];
+    q[LX + 1] = xb[1];
+    q[LLP] = lpb[0];
+    q[LLP + 1] = lpb[1];
+    q[LF] = Fob[0][0];
+    q[LF + 1] = Fob[0][1];
+    q[LF + 2] = Fob[1][0];
+    q[LF + 3] = Fob[1][1];
+    q[LF + 4] = Fob[2][2];
+    q[LB] = bob[0][0];
+    q[LB + 1] = bob[0][1] + bob[1][0];
+    q[LB + 2] = bob[1][1];
+    q[LB + 3] = bob[2][2];
+    q[LE] = Eb;
+    q[LH] = Hb[0][0];
+    q[LH + 1] = Hb[0][1];
+    q[LH + 2] = Hb[1][0];
+    q[LH + 3] = Hb[1][1];
+    q[LU] = ubarb;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -433,7 +559,7 @@ __device__ __forceinline__ void gather_du(const LaunchConst &c, const PtrsP &p, 
 
 // Trial left Cauchy-Green tensor f b_old f^T of the particle (values), with
 // f = I + H and H = sum_a du_a (x) grad N_a over the slots inside the grid:
-// the value part of the passes' kinematics.
+// the values of the kinematics (gathered before the constitutive Jacobian).
 __device__ __forceinline__ void trial_b(const LaunchConst &c, const double *xv, const double *lpv,
                                         const double *bo_v, const double du[9][2], double B[3][3]) {
     const gw_grid_t &g = c.g;
@@ -457,11 +583,11 @@ __device__ __forceinline__ void trial_b(const LaunchConst &c, const double *xv, 
     congruence3(f, bo, B);
 }
 
-// Runs the chunked passes over inputs [0, n_inputs): q[i] = ds / d input_i.
+// q[i] = ds / d input_i for the particle's 19 inputs (external loads, E and the
+// constitutive Jacobian gathered first).
 template <int MODEL>
-__device__ __forceinline__ void adjoint_passes(const LaunchConst &c, const PtrsP &p, int pid, const double du[9][2],
-                                               const DualWeights &wt, int n_inputs, double q[kAdjInputs],
-                                               SolidDual &o) {
+__device__ __forceinline__ void particle_vjp(const LaunchConst &c, const PtrsP &p, int pid, const double du[9][2],
+                                             const VjpWeights &wt, double q[kAdjInputs], ParticleAdj &o) {
     const double E = p.E ? p.E[pid] : c.E0;
     const double ramp = (c.st.current_step + 1.0) / c.st.total_steps;
     const bool ext = p.ext_flag && p.ext_flag[pid];
@@ -473,14 +599,8 @@ __device__ __forceinline__ void adjoint_passes(const LaunchConst &c, const PtrsP
         trial_b(c, p.x + pid * 2, p.lp + pid * 2, p.b_old + (size_t)pid * 9, du, B);
         constitutive_jac<MODEL>(c, model, B, E, wt.x != nullptr, cj);
     }
-#pragma unroll 1
-    for (int off = 0; off < n_inputs; off += kAdjChunk) {
-        solid2d_dual<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E,
-                            fext, du, off, wt, cj, o);
-#pragma unroll
-        for (int l = 0; l < kAdjChunk; ++l)
-            if (off + l < kAdjInputs) q[off + l] = o.s.d[l];
-    }
+    solid2d_vjp<MODEL>(c, p.x + pid * 2, p.lp + pid * 2, p.F_old + (size_t)pid * 9, p.b_old + (size_t)pid * 9, E, fext,
+                       du, wt, cj, q, o);
 }
 
 // Adjoint G2P: seeds (x_new, lp_new, F_new, b_new) bars -> q_bar (written) and
@@ -493,15 +613,15 @@ __global__ void k_adjoint_g2p(LaunchConst c, PtrsP p, const double *__restrict__
     if (pid >= p.n) return;
     double du[9][2];
     gather_du(c, p, pid, u_new, u_old, du);
-    DualWeights wt;
+    VjpWeights wt;
     wt.r = nullptr;
     wt.x = seed_in.x + pid * 2;
     wt.lp = seed_in.lp + pid * 2;
     wt.F = seed_in.F + (size_t)pid * 9;
     wt.b = seed_in.b + (size_t)pid * 9;
     double q[kAdjInputs];
-    SolidDual o;
-    adjoint_passes<MODEL>(c, p, pid, du, wt, kAdjInputs, q, o);
+    ParticleAdj o;
+    particle_vjp<MODEL>(c, p, pid, du, wt, q, o);
     double xb_eff[2];
     for (int k = 0; k < 2; ++k) xb_eff[k] = wt.x[k] + wt.lp[k] * o.xnew_dx[k];
     // particle-input adjoints
@@ -558,12 +678,12 @@ __global__ void k_adjoint_residual(LaunchConst c, PtrsP p, const double *__restr
                 if ((fm >> f) & 1) lam_w[a][f] = lambda_rows[(size_t)row * 2 + f];
         }
     }
-    DualWeights wt;
+    VjpWeights wt;
     wt.r = lam_w;
     wt.x = wt.lp = wt.F = wt.b = nullptr;
     double q[kAdjInputs];
-    SolidDual o;
-    adjoint_passes<MODEL>(c, p, pid, du, wt, LE + 1, q, o);  // inputs x .. E
+    ParticleAdj o;
+    particle_vjp<MODEL>(c, p, pid, du, wt, q, o);  // uses inputs x .. E
     q_out.x[pid * 2] += q[LX];
     q_out.x[pid * 2 + 1] += q[LX + 1];
     q_out.lp[pid * 2] += q[LLP];
