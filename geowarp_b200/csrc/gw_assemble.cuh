@@ -149,8 +149,10 @@ __global__ void __launch_bounds__(32 * kScatterWarps, 6) k_cell_scatter(LaunchCo
     constexpr int NR = NS * NF;             // residual entries of a cell
     constexpr int NB = NS * NS;             // element blocks of a cell
     constexpr int PERB = (NB + 31) / 32;    // blocks per lane
-    __shared__ __align__(16) unsigned char rec_sh[kScatterWarps][RC::BYTES];
-    __shared__ SS ssh[kScatterWarps];
+    constexpr int PB = NF == 2 ? 4 : 2;   // particles staged per batch (static shared memory < 48 KB)
+    __shared__ __align__(16) unsigned char rec_sh[kScatterWarps][PB][RC::BYTES];
+    __shared__ SS ssh[kScatterWarps][PB];
+    __shared__ unsigned char inflag[kScatterWarps][PB][NS];
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     const int ncx = c.g.n_grid[0], ncy = c.g.n_grid[1];
     const int nx3 = (ncx - kx + 2) / 3, ny3 = (ncy - ky + 2) / 3;
@@ -169,107 +171,113 @@ __global__ void __launch_bounds__(32 * kScatterWarps, 6) k_cell_scatter(LaunchCo
         for (int f = 0; f < NF; ++f)
             for (int g = 0; g < NF; ++g) kacc[e][f][g] = 0.0;
     unsigned int touched = 0u;  // bit e: block e of this lane received a contribution
-    unsigned char *sh = rec_sh[wl];
-    SS &s = ssh[wl];
-    // the next particle's record is loaded into registers while the current
-    // one is processed (its global-memory latency overlaps the arithmetic)
-    constexpr int NCH = RC::BYTES / 16, CPL = (NCH + 31) / 32;
-    uint4 nxt[CPL];
-    {
-        const uint4 *src = (const uint4 *)(scratch + (size_t)p0 * RC::BYTES);
-#pragma unroll
-        for (int k = 0; k < CPL; ++k)
-            if (lane + 32 * k < NCH) nxt[k] = src[lane + 32 * k];
-    }
-    for (int t = p0; t < p1; ++t) {
-#pragma unroll
-        for (int k = 0; k < CPL; ++k)
-            if (lane + 32 * k < NCH) ((uint4 *)sh)[lane + 32 * k] = nxt[k];
-        __syncwarp();
-        if (t + 1 < p1) {
-            const uint4 *src = (const uint4 *)(scratch + (size_t)(t + 1) * RC::BYTES);
-#pragma unroll
-            for (int k = 0; k < CPL; ++k)
-                if (lane + 32 * k < NCH) nxt[k] = src[lane + 32 * k];
+    // The cell's particles go in batches of PB: the set-up sections (staging
+    // the records, shape functions, slot weights, columns C_b) run for the
+    // whole batch at once, one (particle, axis / slot) per lane, and the
+    // accumulation then runs over the batch in sorted order, so the sums are
+    // those of one particle at a time.
+    constexpr int NCH = RC::BYTES / 16;
+    for (int t0 = p0; t0 < p1; t0 += PB) {
+        const int np = min(PB, p1 - t0);
+        for (int k = lane; k < np * NCH; k += 32) {
+            const int pp = k / NCH, ch = k % NCH;
+            ((uint4 *)rec_sh[wl][pp])[ch] = ((const uint4 *)(scratch + (size_t)(t0 + pp) * RC::BYTES))[ch];
         }
-        const double *rd = (const double *)sh;
-        const VT *Dm = (const VT *)(rd + RC::ND);
-        const double *Q = rd + 2 * D;
-        const double *fx = rd + 2 * D + L::NQ;
-        if (lane < D) {  // one axis per lane
+        __syncwarp();
+        if (lane < 2 * np) {  // shape functions: one (particle, axis) per lane
+            const int pp = lane >> 1, k = lane & 1;
+            const double *rd = (const double *)rec_sh[wl][pp];
+            SS &s = ssh[wl][pp];
             Axis ax;
-            gimp_axis(rd[lane], rd[D + lane], c.g.h[lane], c.g.inv_h[lane], ax);
-            for (int i = 0; i < 3; ++i) { s.axw[lane][i] = ax.w[i]; s.axg[lane][i] = ax.gw[i]; s.axa[lane][i] = ax.wavg[i]; }
-            s.axoff[lane] = ax.lower - (lane == 0 ? cx : cy);
-            s.axspan[lane] = ax.span;
+            gimp_axis(rd[k], rd[D + k], c.g.h[k], c.g.inv_h[k], ax);
+            for (int i = 0; i < 3; ++i) { s.axw[k][i] = ax.w[i]; s.axg[k][i] = ax.gw[i]; s.axa[k][i] = ax.wavg[i]; }
+            s.axoff[k] = ax.lower - (k == 0 ? cx : cy);
+            s.axspan[k] = ax.span;
         }
         __syncwarp();
-        if (lane < NS) {  // cell slot `lane`: weights (a particle clamped at the grid edge is offset)
-            const int i0 = lane % 3 - s.axoff[0], i1 = lane / 3 - s.axoff[1];
+        for (int k = lane; k < np * NS; k += 32) {  // cell slot weights (a particle clamped at the grid edge is offset)
+            const int pp = k / NS, sl = k % NS;
+            SS &s = ssh[wl][pp];
+            const int i0 = sl % 3 - s.axoff[0], i1 = sl / 3 - s.axoff[1];
             const bool in = i0 >= 0 && i0 < s.axspan[0] && i1 >= 0 && i1 < s.axspan[1];
             const double w0 = in ? s.axw[0][i0] : 0.0, w1 = in ? s.axw[1][i1] : 0.0;
-            s.W[lane] = w0 * w1;
-            s.Wavg[lane] = in ? s.axa[0][i0] * s.axa[1][i1] : 0.0;
-            s.G[lane][0] = in ? s.axg[0][i0] * w1 : 0.0;
-            s.G[lane][1] = in ? w0 * s.axg[1][i1] : 0.0;
-            const unsigned int bits = __ballot_sync(0x1ffu, in);
-            if (lane == 0) s.inspan = bits;
+            s.W[sl] = w0 * w1;
+            s.Wavg[sl] = in ? s.axa[0][i0] * s.axa[1][i1] : 0.0;
+            s.G[sl][0] = in ? s.axg[0][i0] * w1 : 0.0;
+            s.G[sl][1] = in ? w0 * s.axg[1][i1] : 0.0;
+            inflag[wl][pp][sl] = in;
         }
         __syncwarp();
-        if (WANT_K && lane < NS && ((s.inspan >> lane) & 1u)) {  // columns of slot b = lane
-            const int b = lane;
-            const double Wb = s.W[b], Gb0 = s.G[b][0], Gb1 = s.G[b][1];
-            for (int q = 0; q < L::NQ; ++q) {
-                const VT *dq = Dm + q * L::NT;
-                s.C[b][q][0] = (double)dq[L::TH + 0] * Gb0 + (double)dq[L::TH + D] * Gb1;
-                s.C[b][q][1] = (double)dq[L::TH + 1] * Gb0 + (double)dq[L::TH + D + 1] * Gb1 + (double)dq[L::TU] * Wb;
-                if (NF > D)
-                    s.C[b][q][NF - 1] = (double)dq[L::TP] * Wb + (double)dq[L::TD] * (Wb - s.Wavg[b]) +
-                                        (double)dq[L::TG] * Gb0 + (double)dq[L::TG + 1] * Gb1;
-            }
+        if (lane < np) {
+            unsigned int bits = 0u;
+            for (int sl = 0; sl < NS; ++sl) bits |= (unsigned int)inflag[wl][lane][sl] << sl;
+            ssh[wl][lane].inspan = bits;
         }
         __syncwarp();
-        if (lane < NR) {  // residual entry (slot a, field f)
-            const int a = lane / NF, f = lane % NF;
-            if ((s.inspan >> a) & 1u) {
-                const double Wa = s.W[a];
-                double v;
-                if (f < D) {
-                    v = -(s.G[a][0] * Q[L::QU + f] + s.G[a][1] * Q[L::QU + D + f]);
-                    v += Wa * (Q[L::QS] * (f == D - 1 ? gv : 0.0) + fx[f]);
-                    if (f == D - 1) v += Wa * Q[L::QPEN];
-                } else {
-                    v = Wa * Q[L::QM1] + (Wa - s.Wavg[a]) * Q[L::QM3] + s.G[a][0] * Q[L::QM2] + s.G[a][1] * Q[L::QM2 + 1];
+        if (WANT_K)
+            for (int k = lane; k < np * NS; k += 32) {  // columns of slot b of particle pp
+                const int pp = k / NS, b = k % NS;
+                SS &s = ssh[wl][pp];
+                if (!((s.inspan >> b) & 1u)) continue;
+                const VT *Dm = (const VT *)((const double *)rec_sh[wl][pp] + RC::ND);
+                const double Wb = s.W[b], Gb0 = s.G[b][0], Gb1 = s.G[b][1];
+                for (int q = 0; q < L::NQ; ++q) {
+                    const VT *dq = Dm + q * L::NT;
+                    s.C[b][q][0] = (double)dq[L::TH + 0] * Gb0 + (double)dq[L::TH + D] * Gb1;
+                    s.C[b][q][1] = (double)dq[L::TH + 1] * Gb0 + (double)dq[L::TH + D + 1] * Gb1 + (double)dq[L::TU] * Wb;
+                    if (NF > D)
+                        s.C[b][q][NF - 1] = (double)dq[L::TP] * Wb + (double)dq[L::TD] * (Wb - s.Wavg[b]) +
+                                            (double)dq[L::TG] * Gb0 + (double)dq[L::TG + 1] * Gb1;
                 }
-                racc += v;
             }
-        }
-        if (WANT_K) {
-#pragma unroll
-            for (int e = 0; e < PERB; ++e) {
-                const int blk = lane + 32 * e;
-                if (blk >= NB) break;
-                const int a = blk / NS, b = blk % NS;
-                if (!((s.inspan >> a) & 1u) || !((s.inspan >> b) & 1u)) continue;
-                const double Wa = s.W[a], Ga0 = s.G[a][0], Ga1 = s.G[a][1];
-#pragma unroll
-                for (int g = 0; g < NF; ++g) {
-#pragma unroll
-                    for (int f = 0; f < D; ++f) {
-                        double v = -(Ga0 * s.C[b][L::QU + f][g] + Ga1 * s.C[b][L::QU + D + f][g]);
-                        if (f == D - 1) v += Wa * gv * s.C[b][L::QS][g] + Wa * s.C[b][L::QPEN][g];
-                        kacc[e][f][g] -= v;
-                    }
-                    if (NF > D) {
-                        const double v = Wa * s.C[b][L::QM1][g] + (Wa - s.Wavg[a]) * s.C[b][L::QM3][g] +
-                                         Ga0 * s.C[b][L::QM2][g] + Ga1 * s.C[b][L::QM2 + 1][g];
-                        kacc[e][NF - 1][g] -= v;
-                    }
-                }
-                touched |= 1u << e;
-            }
-        }
         __syncwarp();
+        for (int pp = 0; pp < np; ++pp) {
+            const SS &s = ssh[wl][pp];
+            const double *rd = (const double *)rec_sh[wl][pp];
+            const double *Q = rd + 2 * D;
+            const double *fx = rd + 2 * D + L::NQ;
+            if (lane < NR) {  // residual entry (slot a, field f)
+                const int a = lane / NF, f = lane % NF;
+                if ((s.inspan >> a) & 1u) {
+                    const double Wa = s.W[a];
+                    double v;
+                    if (f < D) {
+                        v = -(s.G[a][0] * Q[L::QU + f] + s.G[a][1] * Q[L::QU + D + f]);
+                        v += Wa * (Q[L::QS] * (f == D - 1 ? gv : 0.0) + fx[f]);
+                        if (f == D - 1) v += Wa * Q[L::QPEN];
+                    } else {
+                        v = Wa * Q[L::QM1] + (Wa - s.Wavg[a]) * Q[L::QM3] + s.G[a][0] * Q[L::QM2] + s.G[a][1] * Q[L::QM2 + 1];
+                    }
+                    racc += v;
+                }
+            }
+            if (WANT_K) {
+#pragma unroll
+                for (int e = 0; e < PERB; ++e) {
+                    const int blk = lane + 32 * e;
+                    if (blk >= NB) break;
+                    const int a = blk / NS, b = blk % NS;
+                    if (!((s.inspan >> a) & 1u) || !((s.inspan >> b) & 1u)) continue;
+                    const double Wa = s.W[a], Ga0 = s.G[a][0], Ga1 = s.G[a][1];
+#pragma unroll
+                    for (int g = 0; g < NF; ++g) {
+#pragma unroll
+                        for (int f = 0; f < D; ++f) {
+                            double v = -(Ga0 * s.C[b][L::QU + f][g] + Ga1 * s.C[b][L::QU + D + f][g]);
+                            if (f == D - 1) v += Wa * gv * s.C[b][L::QS][g] + Wa * s.C[b][L::QPEN][g];
+                            kacc[e][f][g] -= v;
+                        }
+                        if (NF > D) {
+                            const double v = Wa * s.C[b][L::QM1][g] + (Wa - s.Wavg[a]) * s.C[b][L::QM3][g] +
+                                             Ga0 * s.C[b][L::QM2][g] + Ga1 * s.C[b][L::QM2 + 1][g];
+                            kacc[e][NF - 1][g] -= v;
+                        }
+                    }
+                    touched |= 1u << e;
+                }
+            }
+        }
+        __syncwarp();  // the next batch reuses the staging buffers
     }
     // exclusive writes: no other cell of this colour touches these rows
     if (lane < NR) {
