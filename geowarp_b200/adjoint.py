@@ -118,7 +118,9 @@ class LoadStepAdjoint:
             AT = e.bsr_struct()
             AT.vals = _p(self._AT)
             self._lam[:n].zero_()
-            it, rr, rc = e.gmres_solve(AT, self._ubar, self._lam, rtol if rtol is not None else e.krylov_rtol)
+            if rtol is None:
+                rtol = max(e.krylov_rtol, e.adjoint_rtol_floor)
+            it, rr, rc = e.gmres_solve(AT, self._ubar, self._lam, rtol)
             if rc not in (L.GW_OK, L.GW_ENOCONV):
                 L.check(rc, "adjoint transpose solve")
             self.last_krylov = (it, rr)

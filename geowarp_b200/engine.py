@@ -121,6 +121,11 @@ class Engine:
         # reference's full solves (the FP64 drop-in)
         self.newton_forcing = 0.1 if precision == "mixed" else None
         self.forcing_max = 0.1
+        # lower bound of the adjoint's transpose-solve tolerance: in mixed
+        # precision the FP32 transposed Jacobian fixes lambda to about 1e-5
+        # relative (the gradient's distance to the FP64 one), so a tighter solve
+        # changes nothing that the FP32 operator resolves
+        self.adjoint_rtol_floor = 1e-5 if precision == "mixed" else 0.0
         self.krylov_max_iter = krylov_max_iter
         if krylov not in ("gmres", "bicgstab"):
             raise ValueError(f"unknown Krylov method {krylov!r}")
