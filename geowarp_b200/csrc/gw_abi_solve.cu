@@ -2,6 +2,7 @@
 // preconditioned flexible GMRES, the workspace-free Krylov entry point and
 // SpMV (declarations and reference citations in include/geowarp_b200.h).
 #include <algorithm>
+#include <type_traits>
 
 #include "gw_host.cuh"
 #include "gw_mg.cuh"
@@ -475,18 +476,13 @@ int mg_numeric(MgHier &h, cudaStream_t s) {
         MgLevel &f = h.lv[l], &c = h.lv[l + 1];
         PtrsA fa = make_ptrs(f.A), ca = make_ptrs(c.A);
         const int nb = c.A.nnzb;
-        if (D == 2) {
-            if (l == 0) k_mg_rap<2, NF, VT><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-            else k_mg_rap<2, NF, double><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-        } else {
-            if (l == 0) k_mg_rap<3, NF, VT><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-            else k_mg_rap<3, NF, double><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
-        }
+        if (D == 2) k_mg_rap<2, NF, VT><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
+        else k_mg_rap<3, NF, VT><<<gw_count_launch(nblk(nb, kThreads)), kThreads, 0, s>>>(f.L, fa, f.fixed, c.L, ca, c.blockrow);
         GW_LAUNCHED();
         const int nrc = c.A.n_rows;
-        k_mg_fix_empty_rows<NF><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca);
-        k_mg_smoother_setup<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, D, c.Minv);
-        k_mg_fixed_mask<NF, double><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, c.fixed);
+        k_mg_fix_empty_rows<NF, VT><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca);
+        k_mg_smoother_setup<NF, VT><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, D, c.Minv);
+        k_mg_fixed_mask<NF, VT><<<gw_count_launch(nblk(nrc, kThreads)), kThreads, 0, s>>>(ca, c.fixed);
         GW_LAUNCHED();
     }
     const int l = h.nl - 1;
@@ -494,8 +490,7 @@ int mg_numeric(MgHier &h, cudaStream_t s) {
     const int n = h.dn;
     GW_CUDA(cudaMemsetAsync(h.dM, 0, 8 * (size_t)n * n, s));
     PtrsA ac = make_ptrs(lc.A);
-    if (l == 0) k_mg_dense_build<NF, VT><<<gw_count_launch(nblk(lc.A.n_rows, kThreads)), kThreads, 0, s>>>(ac, h.dM, n);
-    else k_mg_dense_build<NF, double><<<gw_count_launch(nblk(lc.A.n_rows, kThreads)), kThreads, 0, s>>>(ac, h.dM, n);
+    k_mg_dense_build<NF, VT><<<gw_count_launch(nblk(lc.A.n_rows, kThreads)), kThreads, 0, s>>>(ac, h.dM, n);
     const size_t smem = 8 * (size_t)n * n;
     GW_CUDA(cudaFuncSetAttribute(k_mg_dense_invert, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  8 * kMgCoarseMax * kMgCoarseMax));
@@ -510,15 +505,12 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
     const MgLevel &v = h.lv[l];
     PtrsA a = make_ptrs(v.A);
     const int tb = zero ? kThreads : tune_rows_block();
-    const int g = zero ? red_grid_elems(v.A.n_rows)
-                       : (l == 0 ? resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, v.A.n_rows)
-                                 : resident_rows_grid((const void *)k_mg_jacobi<NF, double>, tb, v.A.n_rows));
+    const int g = zero ? red_grid_elems(v.A.n_rows) : resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, v.A.n_rows);
     // algorithmic bytes: b, x_out, Minv; with a previous iterate also x_in and the matrix
-    const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
+    const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * sizeof(VT) + 4);
     ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
                  2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
-    if (l == 0) k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
-    else k_mg_jacobi<NF, double><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
+    k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
 }
 
 // Largest cluster of the fused coarse tail for this instantiation on the
@@ -563,9 +555,11 @@ int tail_cluster_size(int D) { return D == 2 ? tail_cluster_size<2, NF>() : tail
 // First level of the fused coarse tail (the first coarse level with at most
 // GW_TUNE_MG_TAIL rows), or h.nl - 1 when the tail is off or has no level to
 // smooth.
-template <int NF>
+template <int NF, typename VT>
 int tail_level(const MgHier &h) {
     const int last = h.nl - 1, T = g_tune[GW_TUNE_MG_TAIL];
+    // the fused tail reads FP64 coarse operators: FP64 solves only
+    if (!std::is_same<VT, double>::value) return last;
     if (T <= 0 || last < 2 || tail_cluster_size<NF>(h.lv[0].g.dim) == 0) return last;
     for (int l = 1; l < last; ++l)
         if (h.lv[l].A.n_rows <= T) return l;
@@ -636,7 +630,7 @@ template <int NF, typename VT>
 double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
     const int last = h.nl - 1;
     const int D = h.lv[0].g.dim;
-    const int l0 = tail_level<NF>(h);
+    const int l0 = tail_level<NF, VT>(h);
     double *cur[kMgMaxLevels], *oth[kMgMaxLevels];
     for (int l = 0; l < l0; ++l) {
         const MgLevel &v = h.lv[l], &c = h.lv[l + 1];
@@ -646,18 +640,11 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
             // second separate sweep would have written
             PtrsA a = make_ptrs(v.A);
             const double vs = 8.0 * v.A.n_rows * NF;
-            const double mat = (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4);
+            const double mat = (double)v.A.nnzb * (NF * NF * sizeof(VT) + 4);
             ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
-            if (l == 0)
-                k_mg_presmooth2<NF, VT><<<gw_count_launch(resident_rows_grid(
-                                              (const void *)k_mg_presmooth2<NF, VT>, tune_rows_block(), v.A.n_rows)),
-                                          tune_rows_block(), 0, s>>>(
-                    a, v.Minv, v.b, y, mg_omega(), skip);
-            else
-                k_mg_presmooth2<NF, double><<<gw_count_launch(resident_rows_grid(
-                                                  (const void *)k_mg_presmooth2<NF, double>, tune_rows_block(), v.A.n_rows)),
-                                              tune_rows_block(), 0, s>>>(
-                    a, v.Minv, v.b, y, mg_omega(), skip);
+            k_mg_presmooth2<NF, VT><<<gw_count_launch(resident_rows_grid(
+                                          (const void *)k_mg_presmooth2<NF, VT>, tune_rows_block(), v.A.n_rows)),
+                                      tune_rows_block(), 0, s>>>(a, v.Minv, v.b, y, mg_omega(), skip);
             double *t = x; x = y; y = t;
             for (int it = 2; it < mg_sweeps(l); ++it) {
                 mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
@@ -673,15 +660,10 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         PtrsA a = make_ptrs(v.A), ca = make_ptrs(c.A);
         const double vs = 8.0 * v.A.n_rows * NF;
         {
-        ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * (l == 0 ? sizeof(VT) : 8) + 4));
-        if (l == 0)
-            k_mg_residual<NF, VT><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, VT>,
-                                                                       tune_rows_block(), v.A.n_rows)),
-                                    tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
-        else
-            k_mg_residual<NF, double><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, double>,
-                                                                           tune_rows_block(), v.A.n_rows)),
-                                        tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
+        ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * sizeof(VT) + 4));
+        k_mg_residual<NF, VT><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, VT>,
+                                                                   tune_rows_block(), v.A.n_rows)),
+                                tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
         }
         ProfScope ps(PC_MG_TRANSFER, s, vs + 8.0 * c.A.n_rows * NF);
         if (D == 2)
@@ -839,11 +821,8 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
     {
         const int tb = tune_rows_block();
         (void)resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, 1);
-        (void)resident_rows_grid((const void *)k_mg_jacobi<NF, double>, tb, 1);
         (void)resident_rows_grid((const void *)k_mg_presmooth2<NF, VT>, tb, 1);
-        (void)resident_rows_grid((const void *)k_mg_presmooth2<NF, double>, tb, 1);
         (void)resident_rows_grid((const void *)k_mg_residual<NF, VT>, tb, 1);
-        (void)resident_rows_grid((const void *)k_mg_residual<NF, double>, tb, 1);
         (void)resident_rows_grid((const void *)k_gm_spmv_keep<NF, VT>, kThreads, 1);
     }
     Bump bp{(char *)ws, 0};

@@ -186,7 +186,7 @@ __global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, L
     const int jb = blockIdx.x * blockDim.x + threadIdx.x;
     if (jb >= Ac.nnzb) return;
     const int R = c_blockrow[jb], Rc = Ac.cols[jb];
-    double *out = (double *)Ac.vals + (size_t)jb * NF * NF;
+    VT *out = (VT *)Ac.vals + (size_t)jb * NF * NF;  // the coarse levels store the fine level's value type
     if (!in_range(R, Ac.n_rows, GS_RAP_COARSE) || !in_range(Rc, Ac.n_rows, GS_RAP_COARSE)) {
         for (int q = 0; q < NF * NF; ++q) out[q] = 0.0;
         return;
@@ -252,15 +252,15 @@ __global__ void k_mg_rap(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixed, L
 #pragma unroll
     for (int f = 0; f < NF; ++f)
 #pragma unroll
-        for (int g = 0; g < NF; ++g) out[f * NF + g] = acc[f][g];
+        for (int g = 0; g < NF; ++g) out[f * NF + g] = (VT)acc[f][g];
 }
 
 // coarse rows that received nothing (every child DOF fixed) become identity rows
-template <int NF>
+template <int NF, typename VT>
 __global__ void k_mg_fix_empty_rows(PtrsA A) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= A.n_rows) return;
-    double *vals = (double *)A.vals;
+    VT *vals = (VT *)A.vals;
     int self = -1;
     for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1]; ++j)
         if (A.cols[j] == r) self = j;
@@ -269,8 +269,8 @@ __global__ void k_mg_fix_empty_rows(PtrsA A) {
         bool empty = true;
         for (int j = A.row_ptr[r]; j < A.row_ptr[r + 1] && empty; ++j)
             for (int g = 0; g < NF; ++g)
-                if (vals[(size_t)j * NF * NF + f * NF + g] != 0.0) { empty = false; break; }
-        if (empty) vals[(size_t)self * NF * NF + f * NF + f] = 1.0;
+                if (vals[(size_t)j * NF * NF + f * NF + g] != (VT)0) { empty = false; break; }
+        if (empty) vals[(size_t)self * NF * NF + f * NF + f] = (VT)1;
     }
 }
 

@@ -313,7 +313,8 @@ int gw_bsr_gmres_solve(const gw_bsr_t *A, int32_t prec, int32_t precond, const d
  * gw_bsr_gmres_solve (solvers/quasi_static_solver_2d.py:236-256; the
  * reference's host pyamg path is the closest counterpart).  Hierarchy:
  * factor-2 coarsening per axis, Galerkin coarse operators P^T A P in the same
- * block-CSR layout (FP64), two damped node-block-Jacobi sweeps before and after
+ * block-CSR layout and value type as A (sums in FP64; FP32 values when prec is
+ * GW_PREC_MIXED), two damped node-block-Jacobi sweeps before and after
  * each coarse correction, an explicit dense inverse on the coarsest level
  * (<= 160 unknowns).  Identity rows of A (Dirichlet DOFs) are excluded from the
  * transfer operators.
