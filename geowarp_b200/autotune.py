@@ -3,8 +3,7 @@
 The library's launch shapes and the depth of its multigrid hierarchy are
 process-wide knobs (gw_tune_set): the CTA size of the assembly and of the
 adjoint particle kernels, the warps per CTA of the multigrid row kernels, the
-bound of the dense coarsest level and the row bound of the fused coarse tail
-(levels run as one cluster launch; bitwise the same V-cycle).  Which values are fastest depends on
+bound of the dense coarsest level.  Which values are fastest depends on
 the workload (particle count, material, grid) and on the device, so the
 tuner measures them there: a coordinate search over the knobs, each candidate
 timed with CUDA events on a caller-supplied trial that repeats the same unit
@@ -22,11 +21,12 @@ from . import _lib as L
 # knobs (GW_TUNE_MG_SWEEPS / _OMEGA / _ONE_SWEEP) are not searched: on the
 # workloads here two sweeps at 0.7 on every level were fastest, and damping of
 # 0.8 and above makes the block-Jacobi smoother diverge (GMRES then runs to
-# its iteration cap).
+# its iteration cap).  GW_TUNE_MG_TAIL is not searched either: the fused tail
+# measured slower on every workload, and it runs only in FP64 solves, so a
+# value picked on a mixed-precision trial would be noise.
 KNOBS = {
     "row_warps": (L.TUNE_ROW_WARPS, (2, 4, 8, 16)),
     "mg_coarse": (L.TUNE_MG_COARSE, (40, 80, 160)),
-    "mg_tail": (L.TUNE_MG_TAIL, (0, 512, 4096)),
     "particle_block": (L.TUNE_PARTICLE_BLOCK, (64, 128, 256)),
     "adjoint_block": (L.TUNE_ADJOINT_BLOCK, (64, 128, 256)),
 }

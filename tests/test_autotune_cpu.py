@@ -39,7 +39,7 @@ def test_knob_defaults_and_ranges(lib):
 
 
 def test_coordinate_search_finds_the_separable_optimum(lib):
-    target = {"row_warps": 4, "mg_coarse": 80, "mg_tail": 512, "particle_block": 128, "adjoint_block": 64}
+    target = {"row_warps": 4, "mg_coarse": 80, "particle_block": 128, "adjoint_block": 64}
 
     def cost():
         cfg = autotune.current()
