@@ -259,6 +259,7 @@ struct MgLevel {
     int *tmp, *sws, *blockrow;
     int *child;             // coarse levels: fine rows of the 3^D children of each row (pattern phase)
     int *parent;            // levels with a coarser one: coarse rows of the 2^D parents of each row
+    void *pvals;            // level 0: BF16 copy of the fine Jacobian read by the V-cycle (mixed)
     uint8_t *flags;
 };
 struct MgHier {
@@ -308,6 +309,7 @@ void mg_carve_hier(Bump &bp, MgHier &h, const gw_grid_t &g0, int64_t n_rows0, in
     l0.fixed = (uint8_t *)bp.take(n_rows0);
     const int CN = D == 2 ? 9 : 27, PN = D == 2 ? 4 : 8;
     l0.parent = (int *)bp.take(4 * n_rows0 * PN);
+    l0.pvals = bp.take(2 * n_rows0 * S * nf * nf);
     gw_grid_t g = g0;
     int64_t nodes = g0.n_nodes;
     int l = 0;
@@ -462,6 +464,9 @@ void mg_apply_plan(MgHier &h, const gw_bsr_t *A0, const gw_mg_plan_t *plan, int 
 
 // Numeric phase: smoother blocks and fixed-DOF masks of every level, Galerkin
 // values of the coarse levels, dense inverse of the coarsest.  No host reads.
+template <typename VT>
+inline bool mg_bf16_fine() { return std::is_same<VT, float>::value && g_tune[GW_TUNE_MG_BF16] != 0; }
+
 template <int NF, typename VT>
 int mg_numeric(MgHier &h, cudaStream_t s) {
     const int D = h.lv[0].g.dim;
@@ -505,12 +510,17 @@ void mg_jacobi(const MgHier &h, int l, const double *b, const double *xin, doubl
     const MgLevel &v = h.lv[l];
     PtrsA a = make_ptrs(v.A);
     const int tb = zero ? kThreads : tune_rows_block();
-    const int g = zero ? red_grid_elems(v.A.n_rows) : resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, v.A.n_rows);
+    const bool bf = l == 0 && mg_bf16_fine<VT>();
+    if (bf) a.vals = v.pvals;
+    const int g = zero ? red_grid_elems(v.A.n_rows)
+                       : (bf ? resident_rows_grid((const void *)k_mg_jacobi<NF, __nv_bfloat16>, tb, v.A.n_rows)
+                             : resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, v.A.n_rows));
     // algorithmic bytes: b, x_out, Minv; with a previous iterate also x_in and the matrix
-    const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * sizeof(VT) + 4);
+    const double vs = 8.0 * v.A.n_rows * NF, mat = (double)v.A.nnzb * (NF * NF * (bf ? 2 : sizeof(VT)) + 4);
     ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s,
                  2 * vs + 8.0 * v.A.n_rows * NF * NF + (zero ? 0.0 : vs + mat));
-    k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
+    if (bf) k_mg_jacobi<NF, __nv_bfloat16><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
+    else k_mg_jacobi<NF, VT><<<gw_count_launch(g), tb, 0, s>>>(a, v.Minv, b, xin, xout, mg_omega(), zero, skip);
 }
 
 // Largest cluster of the fused coarse tail for this instantiation on the
@@ -639,12 +649,20 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
             // both zero-start sweeps in one launch, into the buffer the
             // second separate sweep would have written
             PtrsA a = make_ptrs(v.A);
+            const bool bf = l == 0 && mg_bf16_fine<VT>();
+            if (bf) a.vals = v.pvals;
             const double vs = 8.0 * v.A.n_rows * NF;
-            const double mat = (double)v.A.nnzb * (NF * NF * sizeof(VT) + 4);
+            const double mat = (double)v.A.nnzb * (NF * NF * (bf ? 2 : sizeof(VT)) + 4);
             ProfScope ps(l == 0 ? PC_MG_JACOBI : PC_MG_JACOBI_COARSE, s, 2 * vs + 8.0 * v.A.n_rows * NF * NF + mat);
-            k_mg_presmooth2<NF, VT><<<gw_count_launch(resident_rows_grid(
-                                          (const void *)k_mg_presmooth2<NF, VT>, tune_rows_block(), v.A.n_rows)),
-                                      tune_rows_block(), 0, s>>>(a, v.Minv, v.b, y, mg_omega(), skip);
+            if (bf)
+                k_mg_presmooth2<NF, __nv_bfloat16><<<gw_count_launch(resident_rows_grid(
+                                                         (const void *)k_mg_presmooth2<NF, __nv_bfloat16>,
+                                                         tune_rows_block(), v.A.n_rows)),
+                                                     tune_rows_block(), 0, s>>>(a, v.Minv, v.b, y, mg_omega(), skip);
+            else
+                k_mg_presmooth2<NF, VT><<<gw_count_launch(resident_rows_grid(
+                                              (const void *)k_mg_presmooth2<NF, VT>, tune_rows_block(), v.A.n_rows)),
+                                          tune_rows_block(), 0, s>>>(a, v.Minv, v.b, y, mg_omega(), skip);
             double *t = x; x = y; y = t;
             for (int it = 2; it < mg_sweeps(l); ++it) {
                 mg_jacobi<NF, VT>(h, l, v.b, x, y, 0, skip, s);
@@ -660,10 +678,19 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
         PtrsA a = make_ptrs(v.A), ca = make_ptrs(c.A);
         const double vs = 8.0 * v.A.n_rows * NF;
         {
-        ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * sizeof(VT) + 4));
-        k_mg_residual<NF, VT><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, VT>,
-                                                                   tune_rows_block(), v.A.n_rows)),
-                                tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
+        const bool bf = l == 0 && mg_bf16_fine<VT>();
+        PtrsA ar = a;
+        if (bf) ar.vals = v.pvals;
+        ProfScope ps(PC_MG_RESID, s, 3 * vs + (double)v.A.nnzb * (NF * NF * (bf ? 2 : sizeof(VT)) + 4));
+        if (bf)
+            k_mg_residual<NF, __nv_bfloat16><<<gw_count_launch(resident_rows_grid(
+                                                   (const void *)k_mg_residual<NF, __nv_bfloat16>, tune_rows_block(),
+                                                   v.A.n_rows)),
+                                               tune_rows_block(), 0, s>>>(ar, v.b, x, v.r, skip);
+        else
+            k_mg_residual<NF, VT><<<gw_count_launch(resident_rows_grid((const void *)k_mg_residual<NF, VT>,
+                                                                       tune_rows_block(), v.A.n_rows)),
+                                    tune_rows_block(), 0, s>>>(a, v.b, x, v.r, skip);
         }
         ProfScope ps(PC_MG_TRANSFER, s, vs + 8.0 * c.A.n_rows * NF);
         if (D == 2)
@@ -711,7 +738,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
 // instantiated graph serves all Newton iterations of a load step.  The graphs
 // are held in a small cache (least recently used entry replaced).
 struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega, tail;
+    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega, tail, bf16;
     int n_grid[3];
     int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
     gw_bsr_t A;
@@ -766,6 +793,7 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
     k.sweeps = g_tune[GW_TUNE_MG_SWEEPS];
     k.omega = g_tune[GW_TUNE_MG_OMEGA];
     k.tail = g_tune[GW_TUNE_MG_TAIL];
+    k.bf16 = g_tune[GW_TUNE_MG_BF16];
     for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
     for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
     k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;
@@ -823,6 +851,9 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
         (void)resident_rows_grid((const void *)k_mg_jacobi<NF, VT>, tb, 1);
         (void)resident_rows_grid((const void *)k_mg_presmooth2<NF, VT>, tb, 1);
         (void)resident_rows_grid((const void *)k_mg_residual<NF, VT>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_jacobi<NF, __nv_bfloat16>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_presmooth2<NF, __nv_bfloat16>, tb, 1);
+        (void)resident_rows_grid((const void *)k_mg_residual<NF, __nv_bfloat16>, tb, 1);
         (void)resident_rows_grid((const void *)k_gm_spmv_keep<NF, VT>, kThreads, 1);
     }
     Bump bp{(char *)ws, 0};
@@ -855,6 +886,14 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
         // lag: the previous solve's coarse operators, smoothers and dense
         // inverse are still in the workspace; GMRES itself applies A
         rc = (plan_in && plan_in->lag) ? GW_OK : mg_numeric<NF, VT>(h, s);
+        // the V-cycle's BF16 copy of the fine level follows the current A on
+        // every solve, lagged or not (the fine level's own rows are never lagged)
+        if (!rc && mg_bf16_fine<VT>()) {
+            const size_t nv = (size_t)A->nnzb * NF * NF;
+            k_to_bf16<<<gw_count_launch(red_grid_elems((int64_t)nv)), kThreads, 0, s>>>(
+                (const float *)A->vals, (__nv_bfloat16 *)h.lv[0].pvals, nv);
+            GW_LAUNCHED();
+        }
     }
     if (rc) return rc;
     PtrsA a = make_ptrs(*A);

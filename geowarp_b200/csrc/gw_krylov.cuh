@@ -8,6 +8,8 @@
 // immediately once the device "done" flag is set, so the host can enqueue
 // iterations in chunks and poll the flag once per chunk.
 #pragma once
+#include <cuda_bf16.h>
+
 #include "gw_kernels.cuh"
 
 namespace gw {
@@ -88,6 +90,24 @@ __device__ __forceinline__ void load_block(const VT *__restrict__ p, double out[
 #pragma unroll
     for (int i = 0; i < NF * NF; ++i) out[i] = (double)p[i];
 }
+// BF16 blocks (the multigrid's preconditioner copy of a mixed-precision fine
+// level): 2x2 blocks in one 8-byte load, otherwise element by element
+template <int NF>
+__device__ __forceinline__ void load_block_bf16(const __nv_bfloat16 *__restrict__ p, double out[NF * NF]) {
+    if constexpr (NF == 2) {
+        const uint2 u = *reinterpret_cast<const uint2 *>(p);
+        const __nv_bfloat162 a = *reinterpret_cast<const __nv_bfloat162 *>(&u.x);
+        const __nv_bfloat162 b = *reinterpret_cast<const __nv_bfloat162 *>(&u.y);
+        out[0] = __low2float(a); out[1] = __high2float(a); out[2] = __low2float(b); out[3] = __high2float(b);
+    } else {
+#pragma unroll
+        for (int i = 0; i < NF * NF; ++i) out[i] = __bfloat162float(p[i]);
+    }
+}
+template <> __device__ __forceinline__ void load_block<1, __nv_bfloat16>(const __nv_bfloat16 *__restrict__ p, double out[1]) { load_block_bf16<1>(p, out); }
+template <> __device__ __forceinline__ void load_block<2, __nv_bfloat16>(const __nv_bfloat16 *__restrict__ p, double out[4]) { load_block_bf16<2>(p, out); }
+template <> __device__ __forceinline__ void load_block<3, __nv_bfloat16>(const __nv_bfloat16 *__restrict__ p, double out[9]) { load_block_bf16<3>(p, out); }
+template <> __device__ __forceinline__ void load_block<4, __nv_bfloat16>(const __nv_bfloat16 *__restrict__ p, double out[16]) { load_block_bf16<4>(p, out); }
 template <>
 __device__ __forceinline__ void load_block<2, float>(const float *__restrict__ p, double out[4]) {
     const float4 v = *reinterpret_cast<const float4 *>(p);

@@ -506,6 +506,13 @@ __global__ void k_mg_prolong(Lat Lf, PtrsA Af, const uint8_t *__restrict__ ffixe
         if (!((fx >> f) & 1)) xf[(size_t)r * NF + f] += acc[f];
 }
 
+// BF16 copy of FP32 block values (the V-cycle's copy of a mixed-precision
+// fine level; round to nearest)
+__global__ void k_to_bf16(const float *__restrict__ in, __nv_bfloat16 *__restrict__ out, size_t n) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        out[i] = __float2bfloat16_rn(in[i]);
+}
+
 // ---------------------------------------------------------------- transfer lists
 // The transfers above find each child / parent through the lattice
 // (row2node, coordinates, node2row) on every V-cycle.  The pattern phase

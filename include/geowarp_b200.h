@@ -478,6 +478,12 @@ const char *gw_profile_name(int32_t cls);
  *                           one launch per phase); recaptures the step
  *                           graphs.  It pays where the levels are a few
  *                           hundred rows (launch-bound hierarchies)
+ *   GW_TUNE_MG_BF16         1: in mixed-precision multigrid solves the V-cycle
+ *                           reads a BF16 copy of the fine-level Jacobian (made
+ *                           in the numeric phase; GMRES still applies the FP32
+ *                           Jacobian), 0: the FP32 Jacobian (default 1);
+ *                           changes the preconditioner only; recaptures the
+ *                           step graphs
  * MG_SWEEPS and MG_OMEGA change the preconditioner (Krylov iteration counts),
  * not the solution GMRES converges to; they also recapture the step graphs.
  * GS_CANCEL changes the orthogonality of the Krylov basis and so the
@@ -493,7 +499,8 @@ const char *gw_profile_name(int32_t cls);
 #define GW_TUNE_MG_OMEGA 6
 #define GW_TUNE_GS_CANCEL 7
 #define GW_TUNE_MG_TAIL 8
-#define GW_TUNE_COUNT 9
+#define GW_TUNE_MG_BF16 9
+#define GW_TUNE_COUNT 10
 int gw_tune_set(int32_t knob, int32_t value);
 int32_t gw_tune_get(int32_t knob);
 
