@@ -124,8 +124,16 @@ void launch_particle_q(const LaunchConst &c, const PtrsP &p, const int *perm, co
 template <int KIND, bool WANT_K, typename VT>
 int assemble_sorted(const LaunchConst &c, const PtrsP &p, const int *perm, const int *keys, const uint8_t *fm,
                     const double *un, const double *uo, const gw_bsr_t *A, double *R, double *force, const PtrsA &a,
-                    char *ws, cudaStream_t s) {
+                    char *ws, int64_t ws_bytes, cudaStream_t s) {
     const int ncx = c.g.n_grid[0], ncy = c.g.n_grid[1], nc = ncx * ncy;
+    // the records written below must fit the caller's workspace (record size
+    // of this instantiation, not of another precision)
+    const int64_t need = 2 * align256(4 * (int64_t)nc) + (int64_t)QRecord<KIND, VT>::BYTES * p.n;
+    if (need > ws_bytes) {
+        snprintf(g_msg, sizeof(g_msg), "gw_assemble_sorted: workspace of %lld bytes, %lld needed",
+                 (long long)ws_bytes, (long long)need);
+        return GW_EINVAL;
+    }
     int *cstart = (int *)ws;
     int *cend = (int *)(ws + align256(4 * (int64_t)nc));
     unsigned char *scratch = (unsigned char *)(ws + 2 * align256(4 * (int64_t)nc));
@@ -157,12 +165,18 @@ int assemble_sorted(const LaunchConst &c, const PtrsP &p, const int *perm, const
 template <int KIND>
 int assemble_sorted_kind(const LaunchConst &c, const PtrsP &p, const int *perm, const int *keys, const uint8_t *fm,
                          const double *un, const double *uo, const gw_bsr_t *A, int prec, double *R, double *force,
-                         const PtrsA &a, char *ws, cudaStream_t s) {
+                         const PtrsA &a, char *ws, int64_t ws_bytes, cudaStream_t s) {
     int rc;
     if (p.n > 0) {
-        if (!A->vals) rc = assemble_sorted<KIND, false, double>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, s);
-        else if (prec == GW_PREC_F64) rc = assemble_sorted<KIND, true, double>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, s);
-        else rc = assemble_sorted<KIND, true, float>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, s);
+        // residual only (A->vals NULL) keeps the record layout of prec: the
+        // workspace was sized for it (gw_assemble_workspace_bytes)
+        const bool f64 = prec == GW_PREC_F64;
+        if (!A->vals)
+            rc = f64 ? assemble_sorted<KIND, false, double>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, ws_bytes, s)
+                     : assemble_sorted<KIND, false, float>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, ws_bytes, s);
+        else
+            rc = f64 ? assemble_sorted<KIND, true, double>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, ws_bytes, s)
+                     : assemble_sorted<KIND, true, float>(c, p, perm, keys, fm, un, uo, A, R, force, a, ws, ws_bytes, s);
         if (rc) return rc;
     }
     if (A->vals && A->n_rows > 0) {
@@ -211,6 +225,6 @@ extern "C" int gw_assemble_sorted(const gw_grid_t *grid, const gw_material_t *ma
     GW_CUDA(cudaMemsetAsync(R_rows, 0, sizeof(double) * (size_t)A->n_rows * A->nf, s));
     char *ws = (char *)workspace;
     if (grid->kind == GW_KIND_SOLID2D)
-        return assemble_sorted_kind<GW_KIND_SOLID2D>(c, p, perm, keys, free_mask, u_new, u_old, A, prec, R_rows, force, a, ws, s);
-    return assemble_sorted_kind<GW_KIND_COUPLED2D>(c, p, perm, keys, free_mask, u_new, u_old, A, prec, R_rows, force, a, ws, s);
+        return assemble_sorted_kind<GW_KIND_SOLID2D>(c, p, perm, keys, free_mask, u_new, u_old, A, prec, R_rows, force, a, ws, workspace_bytes, s);
+    return assemble_sorted_kind<GW_KIND_COUPLED2D>(c, p, perm, keys, free_mask, u_new, u_old, A, prec, R_rows, force, a, ws, workspace_bytes, s);
 }

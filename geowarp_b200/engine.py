@@ -126,6 +126,12 @@ class Engine:
         # relative (the gradient's distance to the FP64 one), so a tighter solve
         # changes nothing that the FP32 operator resolves
         self.adjoint_rtol_floor = 1e-5 if precision == "mixed" else 0.0
+        # chord final update (mixed precision only): when the residual norms so
+        # far predict ||R|| < tol at the next iterate, that iterate is checked
+        # with a residual-only assembly first; if it has converged, the last
+        # update (solved only to forcing_max) reuses the previous Jacobian
+        # instead of assembling a new tangent
+        self.final_chord = precision == "mixed"
         self.krylov_max_iter = krylov_max_iter
         if krylov not in ("gmres", "bicgstab"):
             raise ValueError(f"unknown Krylov method {krylov!r}")
@@ -495,14 +501,30 @@ class Engine:
         With line_search_growth set (extension, off by default), an iterate
         whose residual norm exceeds growth x the previous one is rejected and
         the previous Newton step is halved (at most line_search_max times per
-        load step); accepted iterates follow the reference exactly."""
+        load step); accepted iterates follow the reference exactly.
+
+        With final_chord (mixed precision), the last update -- taken at
+        ||R|| < tol -- may use the previous iterate's Jacobian: see
+        Engine.__init__."""
         its = 0
         growth = self.line_search_growth
         prev = None  # (u before the last step, delta, ||R|| at u)
         n_bt = 0
         alpha = 1.0
         n = self.n_rows * self.nf
+        norms = []  # ||R|| of the accepted iterates
         for it in range(n_iter):
+            if (self.final_chord and not growth and len(norms) >= 2 and 0.0 < norms[-1] < norms[-2]
+                    and norms[-1] * (norms[-1] / norms[-2]) < 0.5 * tol):
+                self.assemble(mat_struct, current_step, total_steps, want_K=False)
+                self.residual_norm_async()
+                nrm = float(self.norm_dev.item())
+                if nrm < tol:  # converged: the last update with the Jacobian already assembled
+                    kit, relres, rc = self.krylov(self.newton_rtol(nrm, tol))
+                    self.apply_increment()
+                    its += 1
+                    self.log.append((current_step, it, nrm, kit, relres, rc))
+                    break
             self.assemble(mat_struct, current_step, total_steps, want_K=True)
             self.residual_norm_async()
             nrm = float(self.norm_dev.item())
@@ -525,6 +547,7 @@ class Engine:
                 alpha = 1.0
             self.apply_increment()
             its += 1
+            norms.append(nrm)
             self.log.append((current_step, it, nrm, kit, relres, rc))
             if not math.isfinite(nrm):
                 hist = "; ".join(f"it {l[1]}: |R|={l[2]:.3e} krylov {l[3]} relres {l[4]:.2e} rc {l[5]}"

@@ -159,3 +159,28 @@ def test_sort_is_stable_and_deterministic(cuda):
     key = cx + cy * s.n_grid_x
     assert np.array_equal(np.argsort(key, kind="stable"), p1)
     assert np.array_equal(key[p1], k1)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_residual_only_assembly_matches_full(cuda, precision):
+    """A residual-only deterministic assembly (no tangent) gives the bytes of
+    the full assembly's residual, in both precisions.  In mixed precision its
+    records use the FP32-tangent layout the workspace is sized for (an earlier
+    build wrote FP64-layout records there and overran it)."""
+    from geowarp_b200 import batch
+    sizes = [(40, 32), (48, 40)]
+    bb = batch.BatchedBlocks(sizes, logE=batch.random_fields(sizes, seed=5), precision=precision, device="cuda")
+    s = bb.solver
+    e = s.engine
+    for k in range(2):
+        s.advance_one_step(k, 20)
+    s._set_step_params()
+    s.reset()
+    e.sort_and_activate()
+    e.build_system()
+    n = e.n_rows * e.nf
+    e.assemble(s._mat, 2, 20, want_K=True)
+    r_full = e._R[:n].clone()
+    e.assemble(s._mat, 2, 20, want_K=False)
+    torch.cuda.synchronize()
+    assert torch.equal(e._R[:n], r_full)
