@@ -17,7 +17,7 @@ PREC_F64, PREC_F32 = 0, 1
 PRECOND_DIAG, PRECOND_BLOCK = 0, 1
 KRYLOV_BICGSTAB, KRYLOV_CG, KRYLOV_GMRES = 0, 1, 2
 (TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_MG_ONE_SWEEP, TUNE_MG_SWEEPS,
- TUNE_MG_OMEGA, TUNE_GS_CANCEL, TUNE_MG_TAIL, TUNE_MG_BF16, TUNE_COUNT) = range(11)
+ TUNE_MG_OMEGA, TUNE_GS_CANCEL, TUNE_MG_TAIL, TUNE_MG_BF16, TUNE_MG_FINE_SWEEPS, TUNE_COUNT) = range(12)
 
 
 class GeoWarpError(RuntimeError):

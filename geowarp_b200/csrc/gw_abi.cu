@@ -332,6 +332,9 @@ extern "C" int gw_tune_set(int32_t knob, int32_t value) {
         case GW_TUNE_MG_BF16:
             if (value < 0 || value > 1) return GW_EINVAL;
             break;
+        case GW_TUNE_MG_FINE_SWEEPS:
+            if (value < 1 || value > 4) return GW_EINVAL;
+            break;
         default:
             return GW_EINVAL;
     }

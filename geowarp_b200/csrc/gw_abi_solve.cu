@@ -235,7 +235,10 @@ inline double mg_omega() { return 0.01 * g_tune[GW_TUNE_MG_OMEGA]; }
 // smoothing sweeps before / after the coarse correction: two, or one from
 // level GW_TUNE_MG_ONE_SWEEP down (fewer launches on the latency-bound coarse
 // levels against more Krylov iterations; the autotuner weighs the two)
-inline int mg_sweeps(int l) { return l >= g_tune[GW_TUNE_MG_ONE_SWEEP] ? 1 : g_tune[GW_TUNE_MG_SWEEPS]; }
+inline int mg_sweeps(int l) {
+    if (l == 0) return g_tune[GW_TUNE_MG_FINE_SWEEPS];
+    return l >= g_tune[GW_TUNE_MG_ONE_SWEEP] ? 1 : g_tune[GW_TUNE_MG_SWEEPS];
+}
 
 // Bump allocator over the caller's workspace; with p == nullptr it only counts,
 // so sizing and carving run the same code.
@@ -738,7 +741,7 @@ double *mg_vcycle(const MgHier &h, const int *skip, cudaStream_t s) {
 // instantiated graph serves all Newton iterations of a load step.  The graphs
 // are held in a small cache (least recently used entry replaced).
 struct MgGraphKey {
-    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega, tail, bf16;
+    int device, nf, vt_bytes, restart, nl, dn, dim, row_warps, one_sweep, sweeps, omega, tail, bf16, fine_sweeps;
     int n_grid[3];
     int n_rows[kMgMaxLevels], nnzb[kMgMaxLevels];
     gw_bsr_t A;
@@ -794,6 +797,7 @@ int mg_step_graph(const MgHier &h, const gw_grid_t &grid, const gw_bsr_t *A, con
     k.omega = g_tune[GW_TUNE_MG_OMEGA];
     k.tail = g_tune[GW_TUNE_MG_TAIL];
     k.bf16 = g_tune[GW_TUNE_MG_BF16];
+    k.fine_sweeps = g_tune[GW_TUNE_MG_FINE_SWEEPS];
     for (int q = 0; q < 3; ++q) k.n_grid[q] = grid.n_grid[q];
     for (int q = 0; q < h.nl; ++q) { k.n_rows[q] = h.lv[q].A.n_rows; k.nnzb[q] = h.lv[q].A.nnzb; }
     k.A = *A; k.ws = ws; k.b = G.b; k.x = G.x; k.z = G.z;

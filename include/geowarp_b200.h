@@ -484,6 +484,10 @@ const char *gw_profile_name(int32_t cls);
  *                           Jacobian), 0: the FP32 Jacobian (default 1);
  *                           changes the preconditioner only; recaptures the
  *                           step graphs
+ *   GW_TUNE_MG_FINE_SWEEPS  block-Jacobi sweeps before and after the coarse
+ *                           correction on the finest level, 1..4 (default 1);
+ *                           changes the preconditioner; recaptures the step
+ *                           graphs
  * MG_SWEEPS and MG_OMEGA change the preconditioner (Krylov iteration counts),
  * not the solution GMRES converges to; they also recapture the step graphs.
  * GS_CANCEL changes the orthogonality of the Krylov basis and so the
@@ -500,7 +504,8 @@ const char *gw_profile_name(int32_t cls);
 #define GW_TUNE_GS_CANCEL 7
 #define GW_TUNE_MG_TAIL 8
 #define GW_TUNE_MG_BF16 9
-#define GW_TUNE_COUNT 10
+#define GW_TUNE_MG_FINE_SWEEPS 10
+#define GW_TUNE_COUNT 11
 int gw_tune_set(int32_t knob, int32_t value);
 int32_t gw_tune_get(int32_t knob);
 

@@ -232,3 +232,27 @@ def test_fused_coarse_tail_is_bitwise_the_per_phase_vcycle(cuda, precision):
     assert rc0 == 0 and rc1 == 0 and it0 == it1
     assert np.array_equal(x0, x1)
     assert n_tail < n_sep
+
+
+def test_mixed_options_change_iterates_not_the_converged_state(cuda):
+    """The mixed-precision engine's chord final update and the V-cycle's BF16
+    fine-level copy change how each load step is solved, not what it
+    converges to: with both on and both off, the bar's displacement and stress
+    after a few load steps agree far below the Newton tolerance's effect."""
+    from geowarp_b200 import _lib as L
+    from geowarp_b200 import problems
+    lib = L.load()
+    default = lib.gw_tune_get(L.TUNE_MG_BF16)
+    out = {}
+    try:
+        for on in (False, True):
+            assert lib.gw_tune_set(L.TUNE_MG_BF16, int(on)) == L.GW_OK
+            s = problems.bar_compaction_2d(precision="mixed", device=cuda, tol=1e-8)
+            s.engine.final_chord = on
+            for k in range(4):
+                s.advance_one_step(k, 20)
+            out[on] = ((s.x_particles - s.x0).cpu().numpy(), s.particle_Cauchy_stress_array.cpu().numpy())
+    finally:
+        lib.gw_tune_set(L.TUNE_MG_BF16, default)
+    assert rel_err(out[True][0], out[False][0]) < 1e-8
+    assert rel_err(out[True][1], out[False][1]) < 1e-8
