@@ -480,10 +480,12 @@ const char *gw_profile_name(int32_t cls);
  *                           hundred rows (launch-bound hierarchies)
  *   GW_TUNE_MG_BF16         1: in mixed-precision multigrid solves the V-cycle
  *                           reads a BF16 copy of the fine-level Jacobian (made
- *                           in the numeric phase; GMRES still applies the FP32
- *                           Jacobian), 0: the FP32 Jacobian (default 1);
- *                           changes the preconditioner only; recaptures the
- *                           step graphs
+ *                           before each solve; GMRES still applies the FP32
+ *                           Jacobian), 0: the FP32 Jacobian (default 0);
+ *                           changes the preconditioner only, and weakens it on
+ *                           ill-conditioned systems solved to small relative
+ *                           residuals (plastic footings): for well-conditioned
+ *                           ones only; recaptures the step graphs
  *   GW_TUNE_MG_FINE_SWEEPS  block-Jacobi sweeps before and after the coarse
  *                           correction on the finest level, 1..4 (default 1);
  *                           changes the preconditioner; recaptures the step

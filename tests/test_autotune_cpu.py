@@ -8,7 +8,7 @@ from geowarp_b200 import autotune
 
 DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160,
             L.TUNE_MG_ONE_SWEEP: 20, L.TUNE_MG_SWEEPS: 2, L.TUNE_MG_OMEGA: 70, L.TUNE_GS_CANCEL: 20,
-            L.TUNE_MG_TAIL: 0, L.TUNE_MG_BF16: 1, L.TUNE_MG_FINE_SWEEPS: 1}
+            L.TUNE_MG_TAIL: 0, L.TUNE_MG_BF16: 0, L.TUNE_MG_FINE_SWEEPS: 1}
 
 
 @pytest.fixture
