@@ -17,7 +17,8 @@ PREC_F64, PREC_F32 = 0, 1
 PRECOND_DIAG, PRECOND_BLOCK = 0, 1
 KRYLOV_BICGSTAB, KRYLOV_CG, KRYLOV_GMRES = 0, 1, 2
 (TUNE_PARTICLE_BLOCK, TUNE_ADJOINT_BLOCK, TUNE_ROW_WARPS, TUNE_MG_COARSE, TUNE_MG_ONE_SWEEP, TUNE_MG_SWEEPS,
- TUNE_MG_OMEGA, TUNE_GS_CANCEL, TUNE_MG_TAIL, TUNE_MG_BF16, TUNE_MG_FINE_SWEEPS, TUNE_COUNT) = range(12)
+ TUNE_MG_OMEGA, TUNE_GS_CANCEL, TUNE_MG_TAIL, TUNE_MG_BF16, TUNE_MG_FINE_SWEEPS, TUNE_GMRES_STALL,
+ TUNE_COUNT) = range(13)
 
 
 class GeoWarpError(RuntimeError):
@@ -122,6 +123,7 @@ SIGNATURES = {
     "gw_bsr_gmres_mg_solve": (C.c_int, [C.POINTER(Grid), C.POINTER(Bsr), I32, C.POINTER(MgPlan), P, P, C.c_double, I32,
                                         I32, P, I64, PI32, PD, P]),
     "gw_gmres_last_reorths": (I32, []),
+    "gw_gmres_last_stalled": (I32, []),
     "gw_bsr_gmres_solve": (C.c_int, [C.POINTER(Bsr), I32, I32, P, P, C.c_double, I32, I32, P, PI32, PD, P]),
     "gw_bsr_spmv": (C.c_int, [C.POINTER(Bsr), I32, P, P, P]),
     "gw_bsr_spmv_t": (C.c_int, [C.POINTER(Bsr), I32, P, P, P]),

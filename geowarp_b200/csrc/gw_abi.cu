@@ -41,7 +41,7 @@ extern "C" const char *gw_status_string(int code) {
         case GW_OK: return "ok";
         case GW_EINVAL: return g_msg[0] ? g_msg : "invalid argument";
         case GW_ECUDA: return g_msg[0] ? g_msg : "CUDA error";
-        case GW_ENOCONV: return "Krylov solver did not reach the tolerance";
+        case GW_ENOCONV: return "Krylov solver did not reach the tolerance (iteration cap or GMRES stagnation)";
         case GW_EBREAKDOWN: return "Krylov breakdown";
         case GW_ENAN: return "non-finite value";
         case GW_ERANGE: return g_msg[0] ? g_msg : "index guard failed: a device index was out of range";
@@ -334,6 +334,9 @@ extern "C" int gw_tune_set(int32_t knob, int32_t value) {
             break;
         case GW_TUNE_MG_FINE_SWEEPS:
             if (value < 1 || value > 4) return GW_EINVAL;
+            break;
+        case GW_TUNE_GMRES_STALL:
+            if (value < 0 || value > 100000) return GW_EINVAL;
             break;
         default:
             return GW_EINVAL;

@@ -3,6 +3,7 @@
 // SpMV (declarations and reference citations in include/geowarp_b200.h).
 #include <algorithm>
 #include <type_traits>
+#include <vector>
 
 #include "gw_host.cuh"
 #include "gw_mg.cuh"
@@ -104,6 +105,31 @@ int krylov_nf(const gw_bsr_t *A, int method, int precond, const double *b, doubl
 namespace {
 // second Gram-Schmidt passes of the last GMRES solve on this host thread
 thread_local int g_last_reorths = 0;
+// whether the last GMRES solve on this host thread stopped on stagnation
+thread_local int g_last_stalled = 0;
+
+// Restarted GMRES can stagnate for good: the true residual at each cycle start
+// stops falling (a preconditioned operator whose field of values contains
+// zero, or a preconditioner too weak for the accuracy asked).  A solve whose
+// residual fell by less than 10% over the last GW_TUNE_GMRES_STALL restart
+// cycles stops there, and returns GW_ENOCONV, instead of running on to
+// max_iter: at that rate 650 more cycles would gain less than a factor 4.
+// 0 turns the check off.
+class StallWatch {
+  public:
+    StallWatch() : window_(g_tune[GW_TUNE_GMRES_STALL]) {}
+    // beta: the true residual norm at the start of a restart cycle
+    bool stalled(double beta) {
+        if (window_ <= 0) return false;
+        hist_.push_back(beta);
+        const size_t n = hist_.size();
+        return n > (size_t)window_ && beta > 0.9 * hist_[n - 1 - window_];
+    }
+
+  private:
+    int window_;
+    std::vector<double> hist_;
+};
 
 // Profiling only: whether column k takes the second Gram-Schmidt pass (read
 // after pass 0), so that the timed pass-1 launches are credited with the bytes
@@ -151,6 +177,8 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
     GScalars h;
     memset(&h, 0, head);
     int first = 1;
+    StallWatch stall;
+    g_last_stalled = 0;
     for (int cycle = 0; cycle < 1000000; ++cycle) {
         k_gm_residual<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, first, rtol);
         k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 1);
@@ -159,6 +187,7 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
         GW_CUDA(cudaMemcpyAsync(&h, G.sc, head, cudaMemcpyDeviceToHost, s));
         GW_CUDA(cudaStreamSynchronize(s));
         if (h.done) break;
+        if (stall.stalled(h.beta)) { g_last_stalled = 1; break; }
         int chunk = 4;
         int kk = 0;  // host-side column estimate (exact until the cycle closes early)
         const double spmv_bytes = (double)A->nnzb * (NF * NF * sizeof(VT) + 4) + 4.0 * (nr + 1) + 16.0 * n;
@@ -170,7 +199,7 @@ int gmres(const gw_bsr_t *A, int precond, const double *b, double *x, double rto
                 { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
                 const int re = prof_reorth(G.sc, s);
                 { ProfScope ps(PC_DOTS, s, re ? vb : 0.0); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, re ? vb + 8.0 * n : 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_UPDATE, s, re ? vb + 8.0 * n : 0.0); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
                 { ProfScope ps(PC_NEXT, s, 8.0 * n * 3 + 8.0 * nr * NF * NF); k_gm_next<NF><<<gw_count_launch(ge), kThreads, 0, s>>>(nr, G, 0); }
             }
             GW_LAUNCHED();
@@ -917,6 +946,8 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
     GScalars hs;
     memset(&hs, 0, head);
     int first = 1;
+    StallWatch stall;
+    g_last_stalled = 0;
     for (int cycle = 0; cycle < 1000000; ++cycle) {
         k_gm_residual<NF, VT><<<gw_count_launch(gr), kThreads, 0, s>>>(a, G, first, rtol);
         k_gm_next_flex<<<gw_count_launch(gv), kThreads, 0, s>>>((size_t)n, G, 1, h.lv[0].b);
@@ -927,6 +958,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
         GW_CUDA(cudaMemcpyAsync(&hs, G.sc, head, cudaMemcpyDeviceToHost, s));
         GW_CUDA(cudaStreamSynchronize(s));
         if (hs.done) break;
+        if (stall.stalled(hs.beta)) { g_last_stalled = 1; break; }
         // Arnoldi steps queued before the next host check: the previous
         // solve's iteration count to start with (Newton solves of a step look
         // alike), then the iterations left at the observed convergence rate.
@@ -956,7 +988,7 @@ int gmres_mg(const gw_grid_t *grid, const gw_bsr_t *A, gw_mg_plan_t *plan_in, co
                 { ProfScope ps(PC_UPDATE, s, vb + 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 0); }
                 const int re = prof_reorth(G.sc, s);
                 { ProfScope ps(PC_DOTS, s, re ? vb : 0.0); k_gm_dots<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
-                { ProfScope ps(PC_UPDATE, s, re ? vb + 8.0 * n : 8.0 * n); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
+                { ProfScope ps(PC_UPDATE, s, re ? vb + 8.0 * n : 0.0); k_gm_update<<<gw_count_launch(gv), kThreads, 0, s>>>(G, 1); }
                 { ProfScope ps(PC_NEXT, s, 8.0 * n * 3); k_gm_next_flex<<<gw_count_launch(gv), kThreads, 0, s>>>((size_t)n, G, 0, h.lv[0].b); }
                 mg_vcycle<NF, VT>(h, skip, s);
             }
@@ -1045,6 +1077,7 @@ extern "C" int gw_mg_plan_build(const gw_grid_t *grid, const gw_bsr_t *A, void *
 }
 
 extern "C" int32_t gw_gmres_last_reorths(void) { return g_last_reorths; }
+extern "C" int32_t gw_gmres_last_stalled(void) { return g_last_stalled; }
 
 extern "C" int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec,
                                      gw_mg_plan_t *plan_host, const double *b, double *x, double rtol,

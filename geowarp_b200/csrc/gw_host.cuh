@@ -125,7 +125,7 @@ static inline bool vec_ok(const gw_bsr_t *A, const void *u, const void *v) {
 
 // launch-shape knobs (gw_tune_set): particle CTA, adjoint CTA, warps per CTA
 // of the multigrid row kernels, bound of the dense coarsest level
-inline int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160, GW_MG_MAX_LEVELS, 2, 70, 20, 0, 0, 1};
+inline int g_tune[GW_TUNE_COUNT] = {256, 128, 8, 160, GW_MG_MAX_LEVELS, 2, 70, 20, 0, 0, 1, 50};
 // block-row kernels: kRowsPerWarp rows per warp (groups of kLPR lanes)
 static inline int tune_rows_grid(int n_rows) {
     const int w = g_tune[GW_TUNE_ROW_WARPS];

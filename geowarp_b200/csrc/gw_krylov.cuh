@@ -760,34 +760,31 @@ __global__ void k_gm_dots(GmresVecs G, int pass) {
     }
 }
 
-// w -= V c (c = H[.][k] on pass 0, h2 on pass 1); pass 1 closes column k
+// w -= V c (c = H[.][k] on pass 0, h2 on pass 1).  The pass that ends the
+// projection closes column k with ||w||, summed as it writes w: pass 0 when
+// k_gm_dots decided against a second pass (pass 1 then has nothing to do),
+// pass 1 otherwise.
 __global__ void k_gm_update(GmresVecs G, int pass) {
     if (G.sc->cycle_done) return;
     GScalars *sc = G.sc;
+    const bool second = sc->reorth;  // set by k_gm_dots pass 0; uniform over the grid
+    if (pass == 1 && !second) return;  // before reading k: pass 0 has advanced it
     const int k = sc->k;
     if (!in_range(k, sc->restart, GS_KRYLOV_K)) return;  // uniform over the grid
     const size_t n = G.n;
-    const bool second = pass == 1 && sc->reorth;  // uniform over the grid
     __shared__ double coef[kGmresMaxRestart + 1];
     for (int i = threadIdx.x; i <= k; i += blockDim.x) coef[i] = pass == 0 ? sc->H[i][k] : sc->h2[i];
     __syncthreads();
     double d[1] = {0.0};
-    if (pass == 0 || second) {
-        for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-            double w = G.w[q];
-            for (int i = 0; i <= k; ++i) w -= coef[i] * G.V[(size_t)i * n + q];
-            G.w[q] = w;
-            d[0] += w * w;
-        }
-    } else {  // no second pass: the norm only
-        for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
-            const double w = G.w[q];
-            d[0] += w * w;
-        }
+    for (size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x) {
+        double w = G.w[q];
+        for (int i = 0; i <= k; ++i) w -= coef[i] * G.V[(size_t)i * n + q];
+        G.w[q] = w;
+        d[0] += w * w;
     }
-    if (pass == 0) return;
+    if (pass == 0 && second) return;  // pass 1 closes the column
     if (grid_reduce<1>(d, G.partials, &sc->ticket) && threadIdx.x == 0) {
-        if (second)
+        if (pass == 1)
             for (int i = 0; i <= k; ++i) sc->H[i][k] += sc->h2[i];
         const double hn = ::sqrt(d[0]);
         sc->wnorm = hn;

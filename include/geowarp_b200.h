@@ -36,7 +36,8 @@ extern "C" {
 #define GW_OK 0
 #define GW_EINVAL -1        /* bad sizes or null pointers                        */
 #define GW_ECUDA -2         /* a CUDA launch or API call failed                  */
-#define GW_ENOCONV -3       /* Krylov iteration cap reached before tolerance     */
+#define GW_ENOCONV -3       /* Krylov iteration cap (or GMRES stagnation stop)
+                               reached before the tolerance                      */
 #define GW_EBREAKDOWN -4    /* Krylov breakdown (rho or omega underflow)         */
 #define GW_ENAN -5          /* non-finite value detected                         */
 #define GW_ERANGE -6        /* a device index guard failed (see gw_guard_read)   */
@@ -366,6 +367,11 @@ int gw_bsr_gmres_mg_solve(const gw_grid_t *grid, const gw_bsr_t *A, int32_t prec
  * only when it cancelled more of the vector's norm than GW_TUNE_GS_CANCEL
  * allows. */
 int32_t gw_gmres_last_reorths(void);
+/* 1 when the last gw_bsr_gmres_solve / gw_bsr_gmres_mg_solve on the calling
+ * host thread stopped on stagnation (GW_ENOCONV before max_iter): its true
+ * residual fell by less than 10% over the last GW_TUNE_GMRES_STALL restart
+ * cycles.  0 otherwise. */
+int32_t gw_gmres_last_stalled(void);
 /* y = A x (x, y FP64 of length n_rows*nf; A values in prec). */
 int gw_bsr_spmv(const gw_bsr_t *A, int32_t prec, const double *x, double *y, void *stream);
 /* y = A^T x. */
@@ -490,6 +496,10 @@ const char *gw_profile_name(int32_t cls);
  *                           correction on the finest level, 1..4 (default 1);
  *                           changes the preconditioner; recaptures the step
  *                           graphs
+ *   GW_TUNE_GMRES_STALL     restart cycles over which a GMRES solve's true
+ *                           residual must fall by 10%, else the solve stops
+ *                           with GW_ENOCONV before max_iter, 0..100000
+ *                           (default 50; 0: off, run to max_iter)
  * MG_SWEEPS and MG_OMEGA change the preconditioner (Krylov iteration counts),
  * not the solution GMRES converges to; they also recapture the step graphs.
  * GS_CANCEL changes the orthogonality of the Krylov basis and so the
@@ -507,7 +517,8 @@ const char *gw_profile_name(int32_t cls);
 #define GW_TUNE_MG_TAIL 8
 #define GW_TUNE_MG_BF16 9
 #define GW_TUNE_MG_FINE_SWEEPS 10
-#define GW_TUNE_COUNT 11
+#define GW_TUNE_GMRES_STALL 11
+#define GW_TUNE_COUNT 12
 int gw_tune_set(int32_t knob, int32_t value);
 int32_t gw_tune_get(int32_t knob);
 

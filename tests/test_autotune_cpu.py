@@ -8,7 +8,8 @@ from geowarp_b200 import autotune
 
 DEFAULTS = {L.TUNE_PARTICLE_BLOCK: 256, L.TUNE_ADJOINT_BLOCK: 128, L.TUNE_ROW_WARPS: 8, L.TUNE_MG_COARSE: 160,
             L.TUNE_MG_ONE_SWEEP: 20, L.TUNE_MG_SWEEPS: 2, L.TUNE_MG_OMEGA: 70, L.TUNE_GS_CANCEL: 20,
-            L.TUNE_MG_TAIL: 0, L.TUNE_MG_BF16: 0, L.TUNE_MG_FINE_SWEEPS: 1}
+            L.TUNE_MG_TAIL: 0, L.TUNE_MG_BF16: 0, L.TUNE_MG_FINE_SWEEPS: 1,
+            L.TUNE_GMRES_STALL: 50}
 
 
 @pytest.fixture
@@ -28,6 +29,7 @@ def test_knob_defaults_and_ranges(lib):
            (L.TUNE_MG_ONE_SWEEP, 0), (L.TUNE_MG_ONE_SWEEP, 21), (L.TUNE_MG_SWEEPS, 5), (L.TUNE_MG_OMEGA, 101),
            (L.TUNE_GS_CANCEL, -1), (L.TUNE_GS_CANCEL, 301), (L.TUNE_MG_TAIL, -1), (L.TUNE_MG_TAIL, (1 << 20) + 1),
            (L.TUNE_MG_BF16, 2), (L.TUNE_MG_FINE_SWEEPS, 0), (L.TUNE_MG_FINE_SWEEPS, 5),
+           (L.TUNE_GMRES_STALL, -1), (L.TUNE_GMRES_STALL, 100001),
            (L.TUNE_COUNT, 1)]
     for k, v in bad:
         assert lib.gw_tune_set(k, v) == L.GW_EINVAL, (k, v)
