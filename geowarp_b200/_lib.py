@@ -129,6 +129,7 @@ SIGNATURES = {
     "gw_bsr_spmv_t": (C.c_int, [C.POINTER(Bsr), I32, P, P, P]),
     "gw_norm2": (C.c_int, [P, I32, P, P, P]),
     "gw_apply_increment": (C.c_int, [C.POINTER(Bsr), P, P, P]),
+    "gw_predict_increment": (C.c_int, [C.POINTER(Bsr), P, P, P, P]),
     "gw_g2p": (C.c_int, [C.POINTER(Grid), C.POINTER(Step), C.POINTER(Particles), P, P, P]),
     "gw_return_map": (C.c_int, [C.POINTER(Material), I32, P, P, P, P, P, P, P, P]),
     "gw_profile_enable": (C.c_int, [I32]),

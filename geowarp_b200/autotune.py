@@ -46,13 +46,23 @@ def apply(config, knobs=KNOBS):
 
 
 def snapshot(engine):
-    """Copies of the particle state a load step reads and writes."""
-    return {n: getattr(engine, n).clone() for n in STATE if getattr(engine, n, None) is not None}
+    """Copies of the particle state a load step reads and writes, and of the
+    engine's Newton predictor (the previous converged increment and its load
+    step), which decides the step's starting iterate."""
+    snap = {n: getattr(engine, n).clone() for n in STATE if getattr(engine, n, None) is not None}
+    u_prev = getattr(engine, "_u_prev", None)
+    snap["_predictor"] = (None if u_prev is None else u_prev.clone(), getattr(engine, "_u_prev_step", None))
+    return snap
 
 
 def restore(engine, snap):
     for n, t in snap.items():
-        getattr(engine, n).copy_(t)
+        if n == "_predictor":
+            u_prev, step = t
+            engine._u_prev = None if u_prev is None else u_prev.clone()
+            engine._u_prev_step = step
+        else:
+            getattr(engine, n).copy_(t)
 
 
 def cuda_timer(fn):

@@ -261,6 +261,16 @@ extern "C" int gw_apply_increment(const gw_bsr_t *A, const double *delta, double
     return GW_OK;
 }
 
+extern "C" int gw_predict_increment(const gw_bsr_t *A, const uint8_t *free_mask, const double *u_prev, double *u_full,
+                                    void *stream) {
+    GW_REQUIRE(A && free_mask && u_prev && u_full && u_prev != u_full);
+    if (A->n_rows == 0) return GW_OK;
+    k_predict_increment<<<gw_count_launch(nblk(A->n_rows, kThreads)), kThreads, 0, S(stream)>>>(
+        A->n_rows, A->nf, A->row2node, free_mask, u_prev, u_full);
+    GW_LAUNCHED();
+    return GW_OK;
+}
+
 // ==================================================================== G2P
 extern "C" int gw_g2p(const gw_grid_t *grid, const gw_step_t *st, const gw_particles_t *pt, const double *u_new,
                       const double *u_old, void *stream) {

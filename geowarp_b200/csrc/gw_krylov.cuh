@@ -577,6 +577,21 @@ __global__ void k_apply_increment(int n_rows, int nf, const int *__restrict__ ro
     for (int f = 0; f < nf; ++f) u[(size_t)node * nf + f] += delta[(size_t)r * nf + f];
 }
 
+// u[node*nf+f] = u_prev[node*nf+f] on the free DOFs of the active rows (bit f
+// of free_mask[node]), 0 on their Dirichlet DOFs; other nodes are not written
+__global__ void k_predict_increment(int n_rows, int nf, const int *__restrict__ row2node,
+                                    const uint8_t *__restrict__ free_mask, const double *__restrict__ u_prev,
+                                    double *__restrict__ u) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rows) return;
+    const int node = row2node[r];
+    const unsigned m = free_mask[node];
+    for (int f = 0; f < nf; ++f) {
+        const size_t i = (size_t)node * nf + f;
+        u[i] = ((m >> f) & 1u) ? u_prev[i] : 0.0;
+    }
+}
+
 }  // namespace
 }  // namespace gw
 

@@ -132,6 +132,17 @@ class Engine:
         # update (solved only to forcing_max) reuses the previous Jacobian
         # instead of assembling a new tangent
         self.final_chord = precision == "mixed"
+        # Newton's starting iterate (mixed precision, 2D solid only): the previous
+        # load step's converged increment on the new step's free DOFs, when the
+        # previous step was current_step - 1 and its Newton loop reached
+        # ||R|| < tol (gw_predict_increment).  Along a
+        # load ramp consecutive increments differ by the change of the response,
+        # so the first residual starts far below the zero iterate's.  The
+        # converged state does not depend on the start; the reference (and the
+        # FP64 drop-in) starts every load step from zero.
+        self.predict_increment = precision == "mixed" and kind == "solid2d"
+        self._u_prev = None  # converged increment of load step _u_prev_step (node-indexed)
+        self._u_prev_step = None
         self.krylov_max_iter = krylov_max_iter
         if krylov not in ("gmres", "bicgstab"):
             raise ValueError(f"unknown Krylov method {krylov!r}")
@@ -504,15 +515,20 @@ class Engine:
         load step); accepted iterates follow the reference exactly.
 
         With final_chord (mixed precision), the last update -- taken at
-        ||R|| < tol -- may use the previous iterate's Jacobian: see
-        Engine.__init__."""
+        ||R|| < tol -- may use the previous iterate's Jacobian; with
+        predict_increment the loop starts from the previous load step's
+        converged increment instead of zero: see Engine.__init__."""
         its = 0
+        if self.predict_increment and self._u_prev is not None and self._u_prev_step == current_step - 1:
+            L.call("gw_predict_increment", C.byref(self.bsr_struct()), _p(self.free_mask), _p(self._u_prev),
+                   _p(self.u_new), self.stream)
         growth = self.line_search_growth
         prev = None  # (u before the last step, delta, ||R|| at u)
         n_bt = 0
         alpha = 1.0
         n = self.n_rows * self.nf
         norms = []  # ||R|| of the accepted iterates
+        converged = False
         for it in range(n_iter):
             if (self.final_chord and not growth and len(norms) >= 2 and 0.0 < norms[-1] < norms[-2]
                     and norms[-1] * (norms[-1] / norms[-2]) < 0.5 * tol):
@@ -524,6 +540,7 @@ class Engine:
                     self.apply_increment()
                     its += 1
                     self.log.append((current_step, it, nrm, kit, relres, rc))
+                    converged = True
                     break
             self.assemble(mat_struct, current_step, total_steps, want_K=True)
             self.residual_norm_async()
@@ -555,7 +572,16 @@ class Engine:
                 raise L.GeoWarpError(L.GW_ENAN, "newton", f"non-finite residual norm at step {current_step} "
                                      f"(device status {self.device_status()}; {hist})")
             if nrm < tol:
+                converged = True
                 break
+        # only a converged increment predicts the next step's: an unconverged
+        # one (Newton at its iteration cap) is no estimate of the solution
+        self._u_prev_step = None
+        if self.predict_increment and converged:
+            if self._u_prev is None or self._u_prev.numel() != self.u_new.numel():
+                self._u_prev = torch.empty_like(self.u_new)
+            self._u_prev.copy_(self.u_new)
+            self._u_prev_step = current_step
         return its
 
     # ------------------------------------------------------------------ host views

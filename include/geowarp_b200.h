@@ -381,6 +381,15 @@ int gw_norm2(const double *v, int32_t n, double *norm_dev, void *workspace, void
 /* u_full[row2node[r]*nf+f] += delta[r*nf+f]: from_increment_to_solution
  * (mpm/mpm_utils.py:1343-1348) restricted to the active rows. */
 int gw_apply_increment(const gw_bsr_t *A, const double *delta, double *u_full, void *stream);
+/* Newton's starting iterate from the previous load step (no counterpart in the
+ * reference, which zeroes the increment at every load step's reset,
+ * solvers/quasi_static_solver_2d.py:144-145):
+ * u_full[row2node[r]*nf+f] = u_prev[...] on the free DOFs of the active rows
+ * (free_mask of gw_compact_rows), 0 on their Dirichlet DOFs.  Nodes outside
+ * the active set are not written (u_full is zero there after a reset).
+ * u_prev and u_full are node-indexed [n_nodes*nf] and must not alias. */
+int gw_predict_increment(const gw_bsr_t *A, const uint8_t *free_mask, const double *u_prev, double *u_full,
+                         void *stream);
 
 /* ------------------------------------------------------------ G2P
  * Replaces G2P_2d / G2P_coupled_2d / G2P_coupled_3d (mpm/mpm_utils.py:1351-1590)
