@@ -702,6 +702,7 @@ __global__ void k_bsr_transpose(gw_grid_t g, PtrsA A, VT *__restrict__ AT) {
     if (r >= A.n_rows) return;
     const int lane = threadIdx.x & 31;
     const int nf = A.nf, node = A.row2node[r];
+    if (!in_range(node, g.n_nodes, GS_TRANSPOSE)) return;
     int ic[3] = {0, 0, 0};
     {
         int q = node;

@@ -233,6 +233,10 @@ __global__ void k_pattern_count(gw_grid_t g, const uint32_t *__restrict__ cell_s
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= n_rows) return;
     const int node = row2node[r];
+    if (!in_range(node, g.n_nodes, GS_PATTERN_FILL)) {
+        counts[r] = 0;
+        return;
+    }
     int ic[3] = {0, 0, 0};
     {
         int q = node;
