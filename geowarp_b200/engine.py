@@ -35,6 +35,11 @@ PRECISIONS = {"fp64": L.PREC_F64, "mixed": L.PREC_F32}
 # u-p mobility: constant k0, or the J-dependent law of Uzuoka & Borja (2012) Eq. 86
 MOBILITY_LAWS = {"constant": 0, "Uzuoka-Borja": 1}
 PRECONDS = {"diag": L.PRECOND_DIAG, "block": L.PRECOND_BLOCK, "mg": "mg"}
+# Models whose load steps always start from zero, even with predict_increment:
+# non-associated Drucker-Prager and softening NorSand, whose incremental problem
+# can lose uniqueness.  There another starting iterate may converge to another
+# branch than the zero start of the FP64 drop-in.
+_NO_PREDICT_MODELS = (L.MODEL_DP, L.MODEL_NORSAND)
 
 
 def _p(t):
@@ -139,7 +144,8 @@ class Engine:
         # load ramp consecutive increments differ by the change of the response,
         # so the first residual starts far below the zero iterate's.  The
         # converged state does not depend on the start; the reference (and the
-        # FP64 drop-in) starts every load step from zero.
+        # FP64 drop-in) starts every load step from zero.  Not for the models of
+        # _NO_PREDICT_MODELS.
         self.predict_increment = precision == "mixed" and kind == "solid2d"
         self._u_prev = None  # converged increment of load step _u_prev_step (node-indexed)
         self._u_prev_step = None
@@ -519,7 +525,8 @@ class Engine:
         predict_increment the loop starts from the previous load step's
         converged increment instead of zero: see Engine.__init__."""
         its = 0
-        if self.predict_increment and self._u_prev is not None and self._u_prev_step == current_step - 1:
+        predict = self.predict_increment and mat_struct.model not in _NO_PREDICT_MODELS
+        if predict and self._u_prev is not None and self._u_prev_step == current_step - 1:
             L.call("gw_predict_increment", C.byref(self.bsr_struct()), _p(self.free_mask), _p(self._u_prev),
                    _p(self.u_new), self.stream)
         growth = self.line_search_growth
@@ -577,7 +584,7 @@ class Engine:
         # only a converged increment predicts the next step's: an unconverged
         # one (Newton at its iteration cap) is no estimate of the solution
         self._u_prev_step = None
-        if self.predict_increment and converged:
+        if predict and converged:
             if self._u_prev is None or self._u_prev.numel() != self.u_new.numel():
                 self._u_prev = torch.empty_like(self.u_new)
             self._u_prev.copy_(self.u_new)
