@@ -55,3 +55,35 @@ def test_coordinate_search_finds_the_separable_optimum(lib):
     assert set(table) == set(autotune.KNOBS)
     n_cands = sum(len(c) for _, c in autotune.KNOBS.values())
     assert len(calls) == n_cands * 4             # one untimed + three timed trials per candidate
+
+
+def test_snapshot_restores_particle_state_and_newton_predictor():
+    """A restored load step repeats the one it was taken before: the snapshot
+    holds the particle state and the Newton predictor (the previous converged
+    increment and its load step), and restoring hands the engine a copy, so the
+    step run after it cannot overwrite the snapshot."""
+    import types
+
+    import torch
+    eng = types.SimpleNamespace(**{n: torch.arange(6, dtype=torch.float64) + i for i, n in enumerate(autotune.STATE)})
+    eng._u_prev = torch.full((4,), 2.0, dtype=torch.float64)
+    eng._u_prev_step = 4
+    snap = autotune.snapshot(eng)
+    for n in autotune.STATE:
+        getattr(eng, n).add_(100.0)
+    eng._u_prev.fill_(-1.0)
+    eng._u_prev_step = 5
+    autotune.restore(eng, snap)
+    for i, n in enumerate(autotune.STATE):
+        assert torch.equal(getattr(eng, n), torch.arange(6, dtype=torch.float64) + i)
+    assert eng._u_prev_step == 4 and torch.equal(eng._u_prev, torch.full((4,), 2.0, dtype=torch.float64))
+    eng._u_prev.fill_(7.0)  # the next step's hold writes into the engine's copy only
+    autotune.restore(eng, snap)
+    assert torch.equal(eng._u_prev, torch.full((4,), 2.0, dtype=torch.float64))
+
+    # an engine without a held increment restores to none
+    eng._u_prev, eng._u_prev_step = None, None
+    snap = autotune.snapshot(eng)
+    eng._u_prev, eng._u_prev_step = torch.zeros(4), 3
+    autotune.restore(eng, snap)
+    assert eng._u_prev is None and eng._u_prev_step is None
