@@ -564,8 +564,13 @@ def oracle_rate(wl, steps=2, budget_s=15.0):
         return 1.0 / sec, th, sample + " (forward load steps; the CPU path has no adjoint)"
     if isinstance(wl, BatchedWorkload):
         # whole blocks of the batch, each a complete load step: the blocks are
-        # independent, so blocks per second is the metric's own unit
+        # independent, so blocks per second is the metric's own unit.  Its
+        # per-particle work runs compiled (oracle/native.py), threads over
+        # particles, so every host core counts.
+        from oracle import native
         from oracle.bench_sample import oracle_batch_sample
+        if native.load() is not None:
+            th = host_threads()
         rate, n, sample = oracle_batch_sample(wl.sizes, wl.logE, wl.n_steps, budget_s=budget_s, threads=th)
         return rate, th, sample
     from oracle.bench_sample import oracle_load_step_sample

@@ -13,6 +13,7 @@ import time
 import numpy as np
 from scipy.sparse.linalg import spsolve
 
+from . import native
 from .mpm import OracleEngine, init_particles_rectangle_2d
 
 
@@ -251,12 +252,15 @@ def batch_block_oracle(nx, ny, logE, dx=0.05, PPD=2, rho=2000.0, gravity=9.81, n
     return o
 
 
-def oracle_batch_sample(sizes, logE, n_steps, budget_s=20.0, threads=1, max_blocks=None):
+def oracle_batch_sample(sizes, logE, n_steps, budget_s=20.0, threads=1, max_blocks=None, compiled=True):
     """Block load steps per second of the batched inverse analysis in the
     oracle: load step 0 (P2G, Newton to the tolerance with complex-step
     tangents and a SciPy sparse direct solve, G2P) of whole blocks, taken in
     the batch's order until budget_s is spent (at least one block).  The
     blocks are independent, so blocks / seconds is the workload's own unit.
+    With compiled (and the library of oracle/native.py built), the
+    per-particle residuals and tangents run compiled, in threads over
+    particles; otherwise in NumPy, threads over the tangent's passes.
     Returns (block load steps per second, blocks run, description)."""
     offs = np.cumsum([0] + [a * b * 4 for a, b in sizes])
     t0 = time.perf_counter()
@@ -267,6 +271,8 @@ def oracle_batch_sample(sizes, logE, n_steps, budget_s=20.0, threads=1, max_bloc
         nx, ny = sizes[n]
         o = batch_block_oracle(nx, ny, logE[offs[n]:offs[n + 1]])
         o.threads = threads
+        o.use_native = compiled
+        used = o.use_native and native.supports(o)
         o.advance_one_step(0, n_steps)
         its.append(o.iters[-1] if o.iters else 0)
         parts += o.N
@@ -276,6 +282,8 @@ def oracle_batch_sample(sizes, logE, n_steps, budget_s=20.0, threads=1, max_bloc
     sec = time.perf_counter() - t0
     desc = (f"load step 0 of {n_steps} (forward: P2G, {np.mean(its):.1f} Newton iterations with complex-step "
             f"tangents and SciPy spsolve, G2P) of blocks 0..{n - 1} of the batch ({parts} particles, sizes "
-            f"{', '.join(f'{a}x{b}' for a, b in sizes[:n])}), NumPy oracle with {threads} host thread(s) for the "
-            f"tangent passes; the CPU path has no adjoint")
+            f"{', '.join(f'{a}x{b}' for a, b in sizes[:n])}), "
+            + (f"oracle with compiled per-particle residuals and tangents (C++, {threads} OpenMP thread(s) over "
+               f"particles)" if used else f"NumPy oracle with {threads} host thread(s) for the tangent passes")
+            + "; the CPU path has no adjoint")
     return n / sec, n, desc

@@ -30,6 +30,7 @@ from scipy.sparse.linalg import spsolve
 from . import gimp as G
 from .eig import eigh3, from_principal
 from . import materials as MT
+from . import native
 
 CS_H = 1e-30  # complex-step size
 
@@ -193,6 +194,9 @@ class OracleEngine:
                  p2g_projection="consistent"):
         self.kind = kind
         self.threads = 1  # host threads for the tangent's complex-step passes (timing runs raise it)
+        # the compiled per-particle residual and tangent (oracle/native.py) for
+        # the cases it covers; off by default, so the tests check the NumPy path
+        self.use_native = False
         self.D = 2 if kind in ("solid2d", "coupled2d") else 3
         self.nf = {"solid2d": 2, "coupled2d": 3, "coupled3d": 4}[kind]
         self.grid = dict(grid)
@@ -443,7 +447,11 @@ class OracleEngine:
         lower, span, W, Gr, Wa, ids, valid = geo
         Un = self.gather(self.u_new, ids, valid)
         Uo = self.gather(self.u_old, ids, valid)
-        r, aux = self.local(Un, Uo, geo, step, n_steps, want_aux=True)
+        nat = self.use_native and native.supports(self)
+        if nat:
+            r, K_loc, aux = native.solid2d_local(self, geo, Un, Uo, step, n_steps, want_K)
+        else:
+            r, aux = self.local(Un, Uo, geo, step, n_steps, want_aux=True)
         free = self.active & ~self.boundary
         A = ids.shape[1]
         R = np.zeros(self.ndof)
@@ -451,7 +459,14 @@ class OracleEngine:
         okd = valid[:, :, None] & free[np.where(valid[:, :, None], dofs, 0)]
         np.add.at(R, dofs[okd], np.real(r)[okd])
         K = None
-        if want_K:
+        if want_K and nat:
+            # the same entries as the complex-step passes below: row (a, f) and
+            # column (b, g) of every particle where both DOFs are free
+            m = okd[:, :, :, None, None] & okd[:, None, None, :, :]
+            rows = [np.broadcast_to(dofs[:, :, :, None, None], m.shape)[m]]
+            cols = [np.broadcast_to(dofs[:, None, None, :, :], m.shape)[m]]
+            vals = [K_loc[m]]
+        elif want_K:
             def column(bg):
                 # complex-step pass for local column (b, g): K = -dR/du
                 b, g = bg
@@ -475,6 +490,7 @@ class OracleEngine:
             rows = [r for r, _, _ in parts]
             cols = [c for _, c, _ in parts]
             vals = [v for _, _, v in parts]
+        if want_K:
             nf_rows = np.where(~free)[0]
             rows.append(nf_rows)
             cols.append(nf_rows)

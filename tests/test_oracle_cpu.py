@@ -174,3 +174,44 @@ def test_threaded_tangent_passes_give_the_same_jacobian():
     R2, K2, _ = o.assemble(0, 100)
     assert np.array_equal(R1, R2)
     assert (K1 != K2).nnz == 0 and K1.nnz == K2.nnz
+
+
+def test_compiled_per_particle_path_matches_the_numpy_oracle():
+    """oracle/solid2d_cpu.cpp (the CPU baseline's per-particle residuals and
+    complex-step tangents) against the NumPy oracle: one assembly from a
+    perturbed state agrees to round-off, and whole load steps of a batch
+    block follow the same Newton iterations to the same state."""
+    from oracle import native
+    from oracle.bench_sample import batch_block_oracle
+    native.build()
+    assert native.load() is not None
+    rng = np.random.default_rng(3)
+    logE = np.log(1e7) + 0.3 * rng.normal(size=14 * 10 * 4)
+
+    o = batch_block_oracle(14, 10, logE)
+    o.advance_one_step(0, 20)  # F, b and x away from the initial state
+    o.u_old[:] = 0.0
+    o.u_new[:] = 0.0
+    o.p2g()
+    free = o.active & ~o.boundary
+    o.u_new[free] = 1e-4 * rng.normal(size=int(free.sum()))
+    assert native.supports(o)
+    R0, K0, a0 = o.assemble(1, 20)
+    o.use_native, o.threads = True, 3
+    R1, K1, a1 = o.assemble(1, 20)
+    assert np.abs(R1 - R0).max() <= 1e-12 * np.abs(R0).max()
+    assert K1.nnz == K0.nnz
+    assert abs(K1 - K0).max() <= 1e-12 * abs(K0).max()
+    for k in ("F_new", "b_new", "sigma"):
+        assert np.abs(a1[k] - np.real(a0[k])).max() <= 1e-12 * np.abs(np.real(a0[k])).max()
+
+    runs = {}
+    for use in (False, True):
+        o = batch_block_oracle(14, 10, logE)
+        o.use_native, o.threads = use, 2
+        for k in range(3):
+            o.advance_one_step(k, 20)
+        runs[use] = (o.x.copy(), o.sigma.copy(), list(o.iters))
+    assert runs[True][2] == runs[False][2]
+    assert np.abs(runs[True][0] - runs[False][0]).max() <= 1e-12 * np.abs(runs[False][0]).max()
+    assert np.abs(runs[True][1] - runs[False][1]).max() <= 1e-9 * np.abs(runs[False][1]).max()
