@@ -462,10 +462,8 @@ class OracleEngine:
         if want_K and nat:
             # the same entries as the complex-step passes below: row (a, f) and
             # column (b, g) of every particle where both DOFs are free
-            m = okd[:, :, :, None, None] & okd[:, None, None, :, :]
-            rows = [np.broadcast_to(dofs[:, :, :, None, None], m.shape)[m]]
-            cols = [np.broadcast_to(dofs[:, None, None, :, :], m.shape)[m]]
-            vals = [K_loc[m]]
+            rr, cc, vv = native.triplets(self, dofs, okd, K_loc)
+            rows, cols, vals = [rr], [cc], [vv]
         elif want_K:
             def column(bg):
                 # complex-step pass for local column (b, g): K = -dR/du

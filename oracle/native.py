@@ -45,6 +45,9 @@ def load():
         f.restype = C.c_int
         f.argtypes = [C.c_int64] + [C.c_void_p] * 7 + [C.c_double] * 4 + [C.c_void_p, C.c_int32, C.c_int32] + \
             [C.c_void_p] * 5
+        t = lib.gw_oracle_triplets
+        t.restype = C.c_int
+        t.argtypes = [C.c_int64] + [C.c_void_p] * 4 + [C.c_int32] + [C.c_void_p] * 3
         _lib = lib
     return _lib
 
@@ -83,3 +86,22 @@ def solid2d_local(o, geo, Un, Uo, step, n_steps, want_K):
     if rc != 0:
         raise RuntimeError("gw_oracle_solid2d_hencky: bad arguments")
     return r, K, dict(F_new=F_new, b_new=b_new, sigma=sigma, pi_new=o.pi_new, force=0.0)
+
+
+def triplets(o, dofs, okd, K):
+    """(rows, cols, vals) of the Jacobian entries whose row and column DOFs
+    are both free, from the element tangents K[N, 9, 2, 9, 2]: the entries
+    and order of the oracle's NumPy masks, listed by the compiled library."""
+    N = dofs.shape[0]
+    d = np.ascontiguousarray(dofs.reshape(N, 18), dtype=np.int64)
+    ok = np.ascontiguousarray(okd.reshape(N, 18), dtype=np.uint8)
+    cnt = ok.sum(1, dtype=np.int64) ** 2
+    offsets = np.zeros(N, dtype=np.int64)
+    np.cumsum(cnt[:-1], out=offsets[1:])
+    total = int(cnt.sum())
+    rows, cols, vals = np.empty(total, np.int64), np.empty(total, np.int64), np.empty(total)
+    rc = load().gw_oracle_triplets(N, _ptr(d), _ptr(ok), _ptr(np.ascontiguousarray(K)), _ptr(offsets),
+                                   int(max(1, o.threads)), _ptr(rows), _ptr(cols), _ptr(vals))
+    if rc != 0:
+        raise RuntimeError("gw_oracle_triplets: bad arguments")
+    return rows, cols, vals

@@ -243,4 +243,30 @@ int gw_oracle_solid2d_hencky(int64_t N, const double *W, const double *Gr, const
     return 0;
 }
 
+// Triplets of the global Jacobian from the element tangents: for every particle
+// n, row (a, f) and column (b, g) whose DOFs are both free (ok[n][a*2+f]), the
+// entry (dofs[n][a*2+f], dofs[n][b*2+g], K[n][a*2+f][b*2+g]), in the order
+// n, (a, f), (b, g) -- the order in which the oracle's NumPy masks list them,
+// so the summed matrix is the same.  offsets[n]: the first output slot of
+// particle n (an exclusive prefix sum of the squared free-DOF counts).
+int gw_oracle_triplets(int64_t N, const int64_t *dofs, const uint8_t *ok, const double *K, const int64_t *offsets,
+                       int32_t threads, int64_t *rows, int64_t *cols, double *vals) {
+    if (N < 0 || !dofs || !ok || !K || !offsets || !rows || !cols || !vals || threads < 1) return -1;
+#pragma omp parallel for num_threads(threads) schedule(static)
+    for (int64_t n = 0; n < N; ++n) {
+        int64_t o = offsets[n];
+        for (int i = 0; i < 18; ++i) {
+            if (!ok[n * 18 + i]) continue;
+            for (int j = 0; j < 18; ++j) {
+                if (!ok[n * 18 + j]) continue;
+                rows[o] = dofs[n * 18 + i];
+                cols[o] = dofs[n * 18 + j];
+                vals[o] = K[n * 324 + i * 18 + j];
+                ++o;
+            }
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"
