@@ -22,9 +22,11 @@ namespace {  // internal linkage: each translation unit compiles the kernels it 
 
 constexpr int ST_RANGE = 1, ST_NAN = 2, ST_BREAKDOWN = 4;
 
-// Index guards.  Every index the solver kernels compute from a row map, a
-// column array, a stencil or a Krylov counter is checked against the extent
-// of the array it addresses before the access.  A failed check skips the
+// Index guards.  Indices the kernels compute from a column array, a stencil,
+// a coarse transfer list or a Krylov counter, and row-map lookups wherever the
+// kernel knows the node count, are checked against the extent of the array
+// they address before the access (the matrix-only kernels trust the fine rows'
+// row2node written by gw_compact_rows).  A failed check skips the
 // access, sets ST_RANGE and records the first failing site and its value
 // (gw_guard_read), so a corrupted pattern surfaces as GW_ERANGE on the host
 // instead of as a memory fault.

@@ -162,10 +162,13 @@ const char *gw_status_string(int code);
 /* Device-side error flag written by kernels (range / NaN); read & clear. */
 int gw_read_device_status(int32_t *flag_host, void *stream);
 /* Index guards (no counterpart in the reference, whose Warp kernels bounds-check
- * in debug mode only): every index the solver kernels derive from a row map,
- * a column array, a stencil or a Krylov counter is checked before use; a
- * failed check skips the access and records the first failing site and
- * value.  The Krylov and multigrid entry points return GW_ERANGE when one
+ * in debug mode only): indices the kernels derive from a column array, a
+ * stencil, a coarse transfer list or a Krylov counter, and row-map lookups
+ * wherever the kernel knows the node count, are checked before use (the
+ * matrix-only kernels -- gw_apply_increment, gw_predict_increment, the
+ * preconditioner set-ups -- trust the fine rows' row2node of
+ * gw_compact_rows); a failed check skips the access and records the first
+ * failing site and value.  The Krylov and multigrid entry points return GW_ERANGE when one
  * fired; gw_guard_read reads and clears the record (site 0: none). */
 int gw_guard_read(int32_t *site, int64_t *value, void *stream);
 const char *gw_guard_site_name(int32_t site);
